@@ -1,0 +1,70 @@
+"""Extract golden S matrices from the reference's example outputs.
+
+Run in a checkout that has the reference project at $MOLSCAT_REF (default
+/root/reference); writes tests/golden/molscat_all_propagators.json.  The
+fixture is committed, so nothing at test time reads the reference tree.
+
+Source: examples/output/molscat-all_propagators.output, runs
+"IPROPS=5" (LDPROP, lines 408-537) and "IPROPS=6" (MDPROP, lines 682-811):
+ITYPE=1, JTOT=10, symmetry block 1, N=12, E=1000 and 900 cm-1, 8072 steps.
+The system definition is examples/input/molscat-all_propagators.input:25-71.
+"""
+import json
+import os
+import re
+import sys
+
+REF = os.environ.get("MOLSCAT_REF", "/root/reference")
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "molscat_all_propagators.json")
+
+
+def parse_runs(text):
+    runs = {}
+    sections = re.split(r"=+ model system: ITYPE=1; (IPROPS=[^=]*?) =+", text)
+    # sections: [pre, label1, body1, label2, body2, ...]
+    for label, body in zip(sections[1::2], sections[2::2]):
+        label = label.strip()
+        blocks = []
+        for m in re.finditer(r"ROW  COL.*?\n((?:\s+\d+\s+\d+\s+\S+\s+\S+\s+\S+\s+\S+\n)+)", body):
+            entries = []
+            for line in m.group(1).strip("\n").split("\n"):
+                f = line.split()
+                entries.append((int(f[0]), int(f[1]), float(f[4]), float(f[5])))
+            blocks.append(entries)
+        steps = [int(x) for x in re.findall(r"PROPAGATED FROM\s+\S+\s+TO\s+\S+\s+IN\s+(\d+)\s+STEPS", body)]
+        runs[label] = {"smatrices": blocks, "nstep": steps}
+    return runs
+
+
+def main():
+    path = os.path.join(REF, "examples", "output", "molscat-all_propagators.output")
+    with open(path) as f:
+        runs = parse_runs(f.read())
+    sel = {}
+    for label, key in (("IPROPS=6", "LDMD"), ("IPROPS=5", "LDJ")):
+        r = runs[label]
+        sel[key] = {
+            "energies_cm": [1000.0, 900.0],
+            "nstep": r["nstep"][:2],
+            "smatrix": [
+                [{"row": a, "col": b, "re": c, "im": d} for (a, b, c, d) in blk]
+                for blk in r["smatrices"][:2]
+            ],
+        }
+    doc = {
+        "source": "examples/output/molscat-all_propagators.output (IPROPS=6 lines 682-811, IPROPS=5 lines 408-537)",
+        "system": {
+            "itype": 1, "ured": 20.0, "be": 30.0, "jlevel": [0, 2, 4, 6],
+            "lambda": [0, 2], "terms": [[[1.0, -12, None], [-2.0, -6, None]], [[-0.2, -6, None]]],
+            "rm": 3.5, "epsil": 50.0, "jtot": 10, "block": 1,
+            "rmin": 0.5, "rmax": 20.0, "steps": 12.0, "irmset": 9, "iscru": True,
+        },
+        "runs": sel,
+    }
+    with open(OUT, "w") as f:
+        json.dump(doc, f, indent=1)
+    print("wrote", OUT, file=sys.stderr)
+
+
+if __name__ == "__main__":
+    main()
