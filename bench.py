@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Benchmark: batched FP64 LDMD (MDPROP) propagations on B200.
+
+Workload (one step = one pass of the hot path over the whole batch): the
+atom + rigid-rotor close-coupling system (URED 4 amu, B 60 cm-1, even
+j = 0..10, LJ 12-6 + anisotropic exp/R^-6 terms), JTOT = 0..80 in both
+parity blocks (161 coupled-channel systems, N = 5..36) at 512 collision
+energies drawn uniformly in 1-500 cm-1 (numpy default_rng(20261203 + rank)),
+each propagated with MDPROP from 2.5 to 40 Angstrom in 4000 steps: 82,432
+propagations per step.  Synthetic seeded inputs of that shape (there is no
+published dataset for this path).
+
+Metric: channel^3*steps/s = sum over propagations of N^3*NSTEP, divided by the
+device time of the step (the whole job; max over ranks).  solves/s and the
+counted FP64 rate ride along.  Multi-GPU: every rank runs its own batch
+(different energy draw); no collective on the data path ("weak").
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "channel^3*steps/s (batched LDMD propagations, FP64)"
+UNIT = "channel^3*steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--energies", type=int, default=512)
+    ap.add_argument("--jmax", type=int, default=80)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# clocks during the timed region
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "power_w_max": max(power) if power else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+# CPU side: the oracle (a C restatement of the reference path) as baseline
+# ----------------------------------------------------------------------------
+def _cpu_worker(args):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    jt, block, energy_cm = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from molscat_b200 import systems as S
+    sysm = S.rotor_system()
+    c = sysm.coupling(jt, block)
+    rmin, rmax = S.ROTOR_RMIN_A / sysm.rm, S.ROTOR_RMAX_A / sysm.rm
+    nstep = S.ROTOR_NSTEP
+    dr = (rmax - rmin) / nstep
+    rtab = O.radial_grid(rmin, dr, nstep)
+    ptab = O.ptable(O.Itype1(ured=sysm.ured, be=sysm.be, jlevel=list(sysm.jlevel), lam=list(sysm.lam),
+                             terms=[list(t) for t in sysm.terms], rm=sysm.rm, epsil=sysm.epsil), rtab)
+    oc = O.Coupling(n=c.n, nham=c.nham, vl=c.vl, eint=c.eint, cent=c.cent)
+    ered = energy_cm * sysm.cm2ru
+    y0 = S.wkb_initial_y(c, ptab[0], rtab[0], ered)
+    t0 = time.perf_counter()
+    _, nodes, st, _ = O.mdprop(oc, rtab, ptab, nstep, dr, ered, y0)
+    dt = time.perf_counter() - t0
+    return c.n ** 3 * nstep, dt, st
+
+
+def cpu_sample_jobs(count: int, seed: int = 7):
+    """A sample of (JTOT, block, E) from the benchmark batch, weighted like it."""
+    import numpy as np
+    from molscat_b200 import systems as S
+    rng = np.random.default_rng(seed)
+    sysm = S.rotor_system()
+    blocks = [(j, b) for j in range(0, 81) for b in (1, 2) if sysm.channels(j, b)]
+    e = S.batched_energies(512)
+    return [(*blocks[rng.integers(len(blocks))], float(e[rng.integers(512)])) for _ in range(count)]
+
+
+def cpu_baseline_serial(budget_s: float):
+    """Single-thread oracle on a bounded sample of the workload."""
+    from oracle import oracle as O
+    O.build()
+    work = tsum = 0.0
+    jobs = 0
+    for job in cpu_sample_jobs(400):
+        w, dt, st = _cpu_worker(job)
+        work += w
+        tsum += dt
+        jobs += 1
+        if tsum > budget_s:
+            break
+    return {"value": work / tsum, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{jobs} full 4000-step MDPROP propagations drawn from the batch, oracle C restatement "
+                      f"(unpivoted SYMINV N<=30, scipy-OpenBLAS DSYTRF/DSYTRI N>30), 1 thread, {tsum:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the reference path's CPU implementation (the oracle
+    port; the Fortran reference cannot be compiled here) on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from oracle import oracle as O
+    O.build()
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    per_step = cores
+    samples = cpu_sample_jobs(per_step * (args.steps + args.warmup), seed=11)
+    times = []
+    work_total = 0.0
+    with ctx.Pool(cores) as pool:
+        for s in range(args.warmup + args.steps):
+            chunk = samples[s * per_step:(s + 1) * per_step]
+            t0 = time.perf_counter()
+            res = pool.map(_cpu_worker, chunk)
+            dt = time.perf_counter() - t0
+            if any(r[2] != 0 for r in res):
+                raise RuntimeError("oracle propagation failed")
+            if s >= args.warmup:
+                times.append(dt)
+                work_total += sum(r[0] for r in res)
+    tt = sum(times)
+    value = work_total / tt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "rotor close-coupling MDPROP, 4000 steps 2.5-40 A; each step = "
+                               f"{per_step} propagations sampled from the JTOT=0..80 x 2 parities x 512 energies batch",
+                   "parallelism": f"{cores} host processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{per_step} full propagations per step, spawn pool of {cores} processes, "
+                                   "OpenBLAS 1 thread each"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# GPU arm
+# ----------------------------------------------------------------------------
+def fp64_peaks(torch):
+    """Measured FP64 peaks on this GPU: cuBLAS DGEMM (burst) and our DFMA probe."""
+    import ctypes
+    from molscat_b200 import _lib
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3))
+    del a, b
+    L = _lib.load()
+    out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream()
+    fl = ctypes.c_double(0.0)
+    bestp = 0.0
+    for it in (200, 2000, 2000):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rc = L.mgpu_probe_fp64_fma(ctypes.c_void_p(out.data_ptr()), it, ctypes.c_void_p(st.cuda_stream),
+                                   ctypes.byref(fl))
+        e1.record()
+        e1.synchronize()
+        if rc != 0:
+            break
+        bestp = max(bestp, fl.value / (e0.elapsed_time(e1) * 1e-3))
+    torch.cuda.empty_cache()
+    return best, bestp
+
+
+def load_traffic():
+    """DRAM bytes per launch of the propagation kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ldmd_prop_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    # CPU baseline first (rank 0, N=1): before CUDA is initialised
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_serial(args.cpu_seconds)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from molscat_b200.build import build
+    if rank == 0:
+        build()
+    if dist:
+        dist.barrier()
+    from molscat_b200 import systems as S
+    from molscat_b200.propagators import Plan
+
+    t_setup = time.perf_counter()
+    wl = S.batched_workload(n_energies=args.energies, jmax=args.jmax, seed=20261203 + rank)
+    plan = Plan("LDMD", wl.systems, wl.segments, wl.job_sys, wl.job_ered)
+    y0_host = plan.pack(wl.job_y0)
+    t_setup = time.perf_counter() - t_setup
+    work = wl.channel3_steps()
+    njobs = wl.njobs
+
+    dev = torch.device("cuda", local)
+    y0_dev = torch.from_numpy(y0_host).to(dev)
+    y_dev = torch.empty_like(y0_dev)
+    nodes = torch.zeros(njobs, dtype=torch.int32, device=dev)
+    status = torch.zeros(njobs, dtype=torch.int32, device=dev)
+    kfail = torch.zeros(njobs, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    ev = []
+
+    def step(record=False):
+        y_dev.copy_(y0_dev)
+        if record:
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            plan.run_device(y_dev.data_ptr(), nodes.data_ptr(), status.data_ptr(), kfail.data_ptr(), sp, phases=1)
+            e[1].record(stream)
+            plan.run_device(y_dev.data_ptr(), nodes.data_ptr(), status.data_ptr(), kfail.data_ptr(), sp, phases=2)
+            e[2].record(stream)
+            ev.append(e)
+        else:
+            plan.run_device(y_dev.data_ptr(), nodes.data_ptr(), status.data_ptr(), kfail.data_ptr(), sp)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    st = status.cpu().numpy()
+    if (st != 0).any():
+        raise RuntimeError(f"{int((st != 0).sum())} propagations failed (first status {int(st[st != 0][0])})")
+
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        step(record=True)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_local = t0.elapsed_time(t1) / args.steps
+    prep_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    prop_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    ms = ms_local
+    if dist:
+        t = torch.tensor([ms_local], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        wt = torch.tensor([work, float(njobs)], dtype=torch.float64, device=dev)
+        dist.all_reduce(wt)
+        work_all, jobs_all = float(wt[0].item()), float(wt[1].item())
+    else:
+        work_all, jobs_all = work, float(njobs)
+
+    # end to end through the C ABI with host buffers (H2D of initial Y, D2H of Y/NODES/status)
+    e2e = None
+    if not args.no_e2e:
+        import ctypes
+        k2 = args.e2e_steps or args.steps
+        plan.run_host(y0_host)  # warm
+        times = []
+        for _ in range(k2):
+            if dist:
+                dist.barrier()
+            ta = time.perf_counter()
+            yh, nd, stt, kf = plan.run_host(y0_host)
+            times.append(time.perf_counter() - ta)
+            if (stt != 0).any():
+                raise RuntimeError("e2e propagation failed")
+        tm = statistics.mean(times)
+        if dist:
+            t = torch.tensor([tm], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tm = float(t.item())
+        e2e = {"value": work_all / tm, "unit": UNIT, "h2d_bytes_per_step": int(plan.y_elems * 8),
+               "d2h_bytes_per_step": int(plan.y_elems * 8 + 3 * 4 * njobs), "solves_per_s": jobs_all / tm,
+               "api": "mgpu_plan_run_host (C ABI, host buffers)"}
+
+    dgemm, dfma = (fp64_peaks(torch) if rank == 0 else (None, None))
+    peak = max(dgemm or 0.0, dfma or 0.0) or None
+    achieved = plan.flops_prop / (prop_ms * 1e-3)
+    traffic = load_traffic()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": work_all / (ms * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "rotor close-coupling (ITYPE=1 style) MDPROP: JTOT=0..%d x 2 parities x %d energies "
+                                   "(1-500 cm-1), 4000 steps 2.5-40 A, N=5..36" % (args.jmax, args.energies),
+                       "systems": len(wl.systems), "propagations_per_gpu": njobs,
+                       "l2": "inputs larger than L2 (2HQ(C) tables %.1f GB)" % (plan.flops_prep and
+                                                                                 sum(16 * (((s.n + 3) // 4) * ((s.n + 3) // 4 + 1) // 2) * 8 * 4000 for s in wl.systems) / 1e9),
+                       "parallelism": "independent batches per GPU (no collective)" if world > 1 else "1 GPU"},
+            "solves_per_s": jobs_all / (ms * 1e-3),
+            "flops_counted_per_s": plan.flops * world / (ms * 1e-3),
+            "gpu_launches": plan.launches * args.steps,
+            "clocks": clk,
+            "roofline": {"bound": "fp64", "kernel": "ldmd_prop_kernel", "achieved": achieved / 1e12,
+                         "peak": (peak or 0) / 1e12, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if peak else None,
+                         "traffic": (traffic or {}).get("bytes_per_launch"),
+                         "peak_source": "max(cuBLAS DGEMM 8192^3, DFMA probe) measured in this run: "
+                                        "dgemm %.1f, dfma %.1f TFLOP/s" % ((dgemm or 0) / 1e12, (dfma or 0) / 1e12),
+                         "algorithmic": "2N^3 + 2 NHAM N(N+1) flops per job step (two inversions + W(B)); "
+                                        "prep kernel N^3 per system step timed separately",
+                         "prop_ms": prop_ms, "prep_ms": prep_ms},
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "setup_s": t_setup,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    plan.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,148 @@
+/*
+ * molscat_gpu.h -- C ABI of the B200 (sm_100a, FP64) log-derivative
+ * propagator library libmolscat_gpu.so.
+ *
+ * It replaces the MOLSCAT / BOUND / FIELD hot path
+ *
+ *   SUBROUTINE MDPROP(N,MXLAM,NHAM,Y,VL,IV,EINT,CENT,RSTART,RSTOP,NSTEP,DR,
+ *                     NODES,IREC,WAVE,ERED,EP2RU,CM2RU,RSCALE,IPRINT)
+ *                                     (source_code/mdprop.f:1-4)
+ *   SUBROUTINE LDPROP(N,MXLAM,NHAM,Z,VL,IV,EINT,CENT,RSTART,RSTOP,NSTEP,DR,
+ *                     NODES,ERED,EP2RU,CM2RU,RSCALE,IPRINT)
+ *                                     (source_code/ldprop.f:1-4)
+ *
+ * and the HAMMAT/SUMLAM/SYMINV work they do per step.  Argument meaning is
+ * unchanged: N channels, Y the N x N column-major log-derivative matrix
+ * (lower triangle read on entry, full symmetric matrix on exit), VL/IV the
+ * coupling array in the reference layout VL(NVLBLK, N(N+1)/2) packed
+ * upper-triangle-by-columns, EINT/CENT the thresholds and L(L+1), ERED the
+ * reduced total energy, DR the step (negative for inward propagation) and
+ * NODES the negative-pivot count.  Everything is in the reference's reduced
+ * units (1/RUNIT^2 energies).
+ *
+ * The only thing that moves across the boundary differently is the
+ * potential: POTENL/SCAPOT/PERTRB/VCONST/EP2RU scaling (hammat.f:37-83) is
+ * user code, so the caller evaluates the P vector that SUMLAM multiplies
+ * into VL at every radius the propagator visits (R_k = RSTART + k*DR/2,
+ * k = 0..2*NSTEP, accumulated as R=R+H like mdprop.f:117,203) and passes
+ * the table.  CENT/R^2, EINT, confinement and -ERED are added on the device
+ * exactly as hammat.f:85-113 does.
+ *
+ * All pointers are plain host pointers unless the name says _dev.  No
+ * CUDA or torch types appear in the signatures.  Return value: MGPU_OK or
+ * one of the MGPU_ERR_* codes; the reference STOPs where these are returned.
+ */
+#ifndef MOLSCAT_GPU_H
+#define MOLSCAT_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (per call and per propagation) */
+#define MGPU_OK 0
+#define MGPU_ERR_INVERSION 1   /* exactly singular pivot: mdprop.f:282-283, ldprop.f:151-153 */
+#define MGPU_ERR_NONFINITE 2   /* NaN/Inf pivot met during an inversion */
+#define MGPU_ERR_ARG 3         /* invalid argument (sizes, null pointers) */
+#define MGPU_ERR_CUDA 4        /* CUDA runtime failure (no device, launch error) */
+#define MGPU_ERR_UNSUPPORTED 5 /* N above the largest compiled bucket */
+#define MGPU_ERR_NOMEM 6       /* device allocation failed */
+#define MGPU_ERR_TIMEOUT 7     /* a bounded in-kernel wait (TMA copy) expired */
+
+/* propagator ids (IPROP values of scctrl.f:170-196) */
+#define MGPU_PROP_LDJ 5  /* Johnson log-derivative, LDPROP */
+#define MGPU_PROP_LDMD 6 /* Manolopoulos diabatic modified log-derivative, MDPROP */
+
+/* One coupled-channel system: a (JTOT, symmetry block[, field]) basis.
+ * Mirrors the arguments and hidden inputs SUMLAM/HAMMAT read
+ * (hammat.f:1-5, sumlam.f:4,22-23). */
+typedef struct mgpu_coupling {
+    int n;              /* N */
+    int nham;           /* NHAM: terms summed into W */
+    int nvlblk;         /* NVLBLK (module potential): stride of VL per pair, >= nham */
+    int ivlfl;          /* IVLFL (COMMON /VLFLAG/): 0 -> P index = term, >0 -> IV */
+    int nconst;         /* NCONST: >0 means EINT is not added (hammat.f:95) */
+    int nrsq;           /* NRSQ: >0 means CENT/R^2 is not added (hammat.f:89) */
+    double conlen;      /* CONLEN: harmonic confinement if > 0 (hammat.f:103-108) */
+    const double *vl;   /* VL(NVLBLK, N(N+1)/2) */
+    const int *iv;      /* IV, same shape as VL, 1-based P indices (ivlfl > 0) */
+    const double *eint; /* EINT(N) */
+    const double *cent; /* CENT(N) */
+} mgpu_coupling;
+
+/* The radial grid of one propagation segment and its potential table. */
+typedef struct mgpu_grid {
+    int nstep;          /* NSTEP */
+    double dr;          /* DR (H = DR/2) */
+    const double *rtab; /* [2*NSTEP+1] radii R_k in visiting order */
+    const double *ptab; /* [2*NSTEP+1][NHAM] P vectors at R_k */
+} mgpu_grid;
+
+/* ---- drop-in single propagations (host buffers) ------------------------
+ * mgpu_mdprop replaces MDPROP with WAVE=.FALSE. and no ISCRU scratch file
+ * (mdprop.f:1-289); mgpu_ldprop replaces LDPROP (ldprop.f:1-154).
+ * y: in = initial log-derivative (lower triangle), out = Y(RSTOP).
+ * *nodes: NODES.  *kfail: 1-based step of a failed inversion, else 0. */
+int mgpu_mdprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
+                double *y, int *nodes, int *kfail);
+int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
+                double *z, int *nodes, int *kfail);
+
+/* ---- batched propagation plans -----------------------------------------
+ * A plan holds many systems and many jobs (one job = one propagation of a
+ * system at one ERED) resident on the device.  For LDMD the energy
+ * independent 2HQ(C) inverses of every step (mdprop.f:113-139; the
+ * reference reuses them across energies through its ISCRU file,
+ * mdprop.f:106-110) are computed once per system and shared by all of its
+ * jobs.  Y buffers hold, job after job in job order, the N*N column-major
+ * matrix of each job (offsets from mgpu_plan_y_offset). */
+typedef struct mgpu_plan mgpu_plan;
+
+int mgpu_plan_create(mgpu_plan **plan, int iprop, int nsys,
+                     const mgpu_coupling *systems, const mgpu_grid *grids,
+                     int njobs, const int *job_sys, const double *job_ered);
+void mgpu_plan_destroy(mgpu_plan *plan);
+size_t mgpu_plan_y_elems(const mgpu_plan *plan);          /* doubles in a Y buffer */
+size_t mgpu_plan_y_offset(const mgpu_plan *plan, int job); /* first double of job */
+double mgpu_plan_flops(const mgpu_plan *plan);            /* counted FP64 work (3N^3+2NHAM N(N+1) per step) */
+
+/* Host buffers: copies Y in, runs every job, copies Y, NODES and status out. */
+int mgpu_plan_run_host(mgpu_plan *plan, double *y, int *nodes, int *status, int *kfail);
+
+/* Device buffers (y_dev in/out, nodes_dev/status_dev/kfail_dev out) on the
+ * given cudaStream_t passed as void* (NULL = legacy default stream).
+ * Asynchronous: returns after the launches are queued. */
+int mgpu_plan_run_device(mgpu_plan *plan, double *y_dev, int *nodes_dev,
+                         int *status_dev, int *kfail_dev, void *stream);
+
+/* As mgpu_plan_run_device, restricted to some phases: bit 0 = the
+ * energy-independent LDMD preparation (2HQ(C) inverses), bit 1 = the
+ * propagation itself.  phases = 3 is a full run.  Lets a caller time the
+ * propagation kernel alone. */
+int mgpu_plan_run_device_phases(mgpu_plan *plan, double *y_dev, int *nodes_dev,
+                                int *status_dev, int *kfail_dev, void *stream,
+                                int phases);
+
+/* The number of kernel launches one run of the plan makes. */
+int mgpu_plan_launches(const mgpu_plan *plan);
+/* FP64 work the propagation phase alone does, and the LDMD preparation alone
+ * (counted like mgpu_plan_flops: N^3 per inversion, 2 NHAM N(N+1) per W). */
+double mgpu_plan_flops_phase(const mgpu_plan *plan, int phases);
+
+/* FP64 FMA throughput probe: `iters` dependent-chain DFMA rounds in every
+ * thread of a full-occupancy grid; *flops_out gets the flops executed.
+ * Launch is asynchronous on `stream`; out_dev (>= 1 double) receives a
+ * checksum so the work cannot be optimised away. */
+int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out);
+
+/* ---- diagnostics --------------------------------------------------------- */
+const char *mgpu_status_string(int status);
+const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */
+int mgpu_max_n(void);                /* largest N the compiled buckets accept */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOLSCAT_GPU_H */

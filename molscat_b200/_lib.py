@@ -1,0 +1,99 @@
+"""ctypes binding of libmolscat_gpu.so (C ABI: include/molscat_gpu.h).
+
+The CUDA library is the only implementation: if it is missing this module
+raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .build import LIB
+
+MGPU_OK = 0
+MGPU_ERR_INVERSION = 1
+MGPU_ERR_NONFINITE = 2
+MGPU_ERR_ARG = 3
+MGPU_ERR_CUDA = 4
+MGPU_ERR_UNSUPPORTED = 5
+MGPU_ERR_NOMEM = 6
+MGPU_ERR_TIMEOUT = 7
+
+MGPU_PROP_LDJ = 5
+MGPU_PROP_LDMD = 6
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Coupling_C(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("nham", ctypes.c_int), ("nvlblk", ctypes.c_int), ("ivlfl", ctypes.c_int),
+        ("nconst", ctypes.c_int), ("nrsq", ctypes.c_int), ("conlen", ctypes.c_double),
+        ("vl", _dp), ("iv", _ip), ("eint", _dp), ("cent", _dp),
+    ]
+
+
+class Grid_C(ctypes.Structure):
+    _fields_ = [("nstep", ctypes.c_int), ("dr", ctypes.c_double), ("rtab", _dp), ("ptab", _dp)]
+
+
+# every symbol include/molscat_gpu.h declares
+EXPORTS = (
+    "mgpu_mdprop", "mgpu_ldprop",
+    "mgpu_plan_create", "mgpu_plan_destroy", "mgpu_plan_y_elems", "mgpu_plan_y_offset",
+    "mgpu_plan_flops", "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
+    "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
+    "mgpu_status_string", "mgpu_last_error", "mgpu_max_n",
+)
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load the CUDA library (no compute call is made)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB
+    if not os.path.exists(p):
+        raise ImportError(f"{p} is missing: build it with `python -m molscat_b200.build` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(p)
+    pc = ctypes.POINTER(Coupling_C)
+    pg = ctypes.POINTER(Grid_C)
+    vp = ctypes.c_void_p
+    L.mgpu_mdprop.argtypes = [pc, pg, ctypes.c_double, _dp, _ip, _ip]
+    L.mgpu_ldprop.argtypes = [pc, pg, ctypes.c_double, _dp, _ip, _ip]
+    L.mgpu_plan_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, pc, pg, ctypes.c_int, _ip, _dp]
+    L.mgpu_plan_destroy.argtypes = [vp]
+    L.mgpu_plan_destroy.restype = None
+    L.mgpu_plan_y_elems.argtypes = [vp]
+    L.mgpu_plan_y_elems.restype = ctypes.c_size_t
+    L.mgpu_plan_y_offset.argtypes = [vp, ctypes.c_int]
+    L.mgpu_plan_y_offset.restype = ctypes.c_size_t
+    L.mgpu_plan_flops.argtypes = [vp]
+    L.mgpu_plan_flops.restype = ctypes.c_double
+    L.mgpu_plan_run_host.argtypes = [vp, _dp, _ip, _ip, _ip]
+    L.mgpu_plan_run_device.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.mgpu_plan_launches.argtypes = [vp]
+    L.mgpu_plan_run_device_phases.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int]
+    L.mgpu_plan_flops_phase.argtypes = [vp, ctypes.c_int]
+    L.mgpu_plan_flops_phase.restype = ctypes.c_double
+    L.mgpu_probe_fp64_fma.argtypes = [vp, ctypes.c_int, vp, _dp]
+    L.mgpu_status_string.argtypes = [ctypes.c_int]
+    L.mgpu_status_string.restype = ctypes.c_char_p
+    L.mgpu_last_error.argtypes = []
+    L.mgpu_last_error.restype = ctypes.c_char_p
+    L.mgpu_max_n.argtypes = []
+    if path is None:
+        _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load().mgpu_last_error().decode()
+
+
+def status_string(code: int) -> str:
+    return load().mgpu_status_string(int(code)).decode()

@@ -1,0 +1,1083 @@
+// libmolscat_gpu: B200 (sm_100a) FP64 log-derivative propagators behind the
+// MDPROP / LDPROP boundary.  C ABI in include/molscat_gpu.h.
+//
+// Kernels (one CTA per matrix, the matrix register-tiled, see tiles.cuh):
+//   ldmd_prep_kernel  energy-independent part of MDPROP: for every step k the
+//                     inverse 2HQ(C_k) = [I/8 - (H^2/48) W_off(C_k)]^-1 - 8I and
+//                     its negative-pivot count (mdprop.f:113-139).  One CTA
+//                     per (system, step): all steps run in parallel.
+//   ldmd_prop_kernel  the sequential MDPROP step loop for one (system, ERED)
+//                     job: reference-potential tan/tanh terms, two symmetric
+//                     inversions, W(B) assembly (mdprop.f:143-230), final
+//                     Y/H (mdprop.f:269-275), NODES (mdprop.f:170,193,279).
+//   ldj_prop_kernel   the LDPROP step loop (ldprop.f:46-147): U and Z are
+//                     inverted together (one barrier per pivot for both).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "molscat_gpu.h"
+#include "tiles.cuh"
+
+namespace mgpu {
+
+constexpr int kT = 4;  // tile edge of every compiled bucket
+constexpr size_t kSmemBudget = 96 * 1024;  // dynamic shared memory per CTA we allow
+
+struct SysDev {
+    int n, nham, ivlfl, nconst, nrsq, nstep, ntiles, pad0;
+    double conlen, dr;
+    const double *vlt;  // [nham][T*T][ntiles] tile layout, zero padding
+    const int *ivt;     // same shape, 0-based P index (ivlfl > 0 only)
+    const double *eint; // [npad]
+    const double *cent; // [npad]
+    const double *rtab; // [2*nstep+1]
+    const double *ptab; // [2*nstep+1][nham]
+    double *q;          // LDMD: [nstep][T*T][ntiles] 2HQ(C_k)
+    int *prep;          // LDMD: [0] negative pivots of all U inversions (NSAVE), [1] status, [2] kfail
+};
+
+struct JobDev {
+    int sys;
+    int out;          // index of the job in the caller's order
+    double ered;
+    long long yoff;   // first double of this job's Y
+};
+
+// W(R) restricted to one tile (HAMMAT + SUMLAM, hammat.f:85-113, sumlam.f).
+// vl points at the [nham][T*T][ntiles] tile array, in shared or global memory.
+// diag_terms=false gives the coupling sum only (what MDPROP's U uses).
+template <int T>
+__device__ __forceinline__ void w_tile(const SysDev &S, const double *__restrict__ vl, int t, int I, int J, int ir,
+                                       double ered, bool diag_terms, double (&w)[T][T])
+{
+    constexpr int TT = T * T;
+    const int nt = S.ntiles;
+    const double *P = S.ptab + (size_t)ir * S.nham;
+#pragma unroll
+    for (int r = 0; r < T; ++r)
+#pragma unroll
+        for (int c = 0; c < T; ++c) w[r][c] = 0.0;
+    if (S.ivlfl <= 0) {
+        for (int l = 0; l < S.nham; ++l) {
+            const double pl = __ldg(P + l);
+            const double *v = vl + (size_t)l * TT * nt + t;
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) w[r][c] = fma(v[(size_t)(r * T + c) * nt], pl, w[r][c]);
+        }
+    } else {
+        for (int l = 0; l < S.nham; ++l) {
+            const double *v = vl + (size_t)l * TT * nt + t;
+            const int *iv = S.ivt + (size_t)l * TT * nt + t;
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) {
+                    const double x = v[(size_t)(r * T + c) * nt];
+                    if (x != 0.0) w[r][c] = fma(x, __ldg(P + __ldg(iv + (size_t)(r * T + c) * nt)), w[r][c]);
+                }
+        }
+    }
+    if (diag_terms && I == J) {
+        const double R = __ldg(S.rtab + ir);
+        double rsq = 1.0 / (R * R);
+        rsq = fmin(rsq, 1.0e16);
+        double conf = 0.0;
+        if (S.conlen > 0.0) {
+            const double c2 = S.conlen * S.conlen;
+            conf = R * R / (c2 * c2);
+        }
+#pragma unroll
+        for (int r = 0; r < T; ++r) {
+            const int i = I * T + r;
+            if (i < S.n) {
+                double x = w[r][r];
+                if (S.nrsq == 0) x += rsq * S.cent[i];
+                if (S.nconst == 0) x += S.eint[i];
+                if (S.conlen > 0.0) x += conf;
+                w[r][r] = x - ered;
+            }
+        }
+    }
+}
+
+// W(R)_ii for one channel (the DIAG array HAMMAT returns).
+template <int T>
+__device__ __forceinline__ double w_diag(const SysDev &S, const double *__restrict__ vl, int i, int ir, double ered)
+{
+    constexpr int TT = T * T;
+    const int nt = S.ntiles;
+    const int I = i / T, r = i - I * T;
+    const int t = I * (I + 1) / 2 + I;
+    const size_t e = (size_t)(r * T + r) * nt + t;
+    const double *P = S.ptab + (size_t)ir * S.nham;
+    double x = 0.0;
+    for (int l = 0; l < S.nham; ++l) {
+        const double v = vl[(size_t)l * TT * nt + e];
+        if (S.ivlfl <= 0) x = fma(v, __ldg(P + l), x);
+        else if (v != 0.0) x = fma(v, __ldg(P + __ldg(S.ivt + (size_t)l * TT * nt + e)), x);
+    }
+    const double R = __ldg(S.rtab + ir);
+    double rsq = fmin(1.0 / (R * R), 1.0e16);
+    if (S.nrsq == 0) x += rsq * S.cent[i];
+    if (S.nconst == 0) x += S.eint[i];
+    if (S.conlen > 0.0) {
+        const double c2 = S.conlen * S.conlen;
+        x += R * R / (c2 * c2);
+    }
+    return x - ered;
+}
+
+// The sector reference-potential solutions of MDPROP (mdprop.f:143-164).
+__device__ __noinline__ void ref_solutions(double wref, double half, double &y14, double &y23)
+{
+    const double arg = half * sqrt(fabs(wref));
+    if (wref < 0.0) {
+        const double tn = tan(arg);
+        y14 = arg / tn - arg * tn;
+        y23 = arg / tn + arg * tn;
+    } else {
+        const double th = tanh(arg);
+        y14 = arg / th + arg * th;
+        y23 = arg / th - arg * th;
+    }
+}
+
+template <int T>
+__device__ __forceinline__ void load_lower(const double *__restrict__ y, int n, int I, int J,
+                                           double (&a)[T][T])
+{
+#pragma unroll
+    for (int r = 0; r < T; ++r)
+#pragma unroll
+        for (int c = 0; c < T; ++c) {
+            const int i = I * T + r, j = J * T + c;
+            const int lo = i < j ? i : j, hi = i < j ? j : i;
+            a[r][c] = (i < n && j < n) ? y[(size_t)lo * n + hi] : 0.0;
+        }
+}
+
+template <int T>
+__device__ __forceinline__ void store_full(double *__restrict__ y, int n, int I, int J, double scale,
+                                          const double (&a)[T][T])
+{
+#pragma unroll
+    for (int r = 0; r < T; ++r)
+#pragma unroll
+        for (int c = 0; c < T; ++c) {
+            const int i = I * T + r, j = J * T + c;
+            if (i < n && j <= i) {
+                const double x = scale * a[r][c];
+                y[(size_t)j * n + i] = x;
+                y[(size_t)i * n + j] = x;
+            }
+        }
+}
+
+// Copy the system's VL tiles into shared memory (once per CTA).
+__device__ __forceinline__ void stage_vl(const SysDev &S, double *__restrict__ dst, int tt, int nthr)
+{
+    const int cnt = S.nham * tt * S.ntiles;
+    for (int i = threadIdx.x; i < cnt; i += nthr) dst[i] = __ldg(S.vlt + i);
+}
+
+// ---------------------------------------------------------------------------
+// MDPROP, energy-independent half: 2HQ(C_k) for every step of every system.
+// grid = (max nstep in bucket, systems in bucket)
+// ---------------------------------------------------------------------------
+template <int T, int NT>
+__global__ void __launch_bounds__(Geom<T, NT>::NTHR, Geom<T, NT>::MINB)
+ldmd_prep_kernel(const SysDev *__restrict__ systems, const int *__restrict__ sys_list)
+{
+    using G = Geom<T, NT>;
+    __shared__ __align__(16) double vb[2 * G::VS];
+    __shared__ SysDev s_sys;
+    if (threadIdx.x == 0) s_sys = systems[sys_list[blockIdx.y]];
+    __syncthreads();
+    const SysDev &S = s_sys;
+    const int k = blockIdx.x + 1;
+    if (k > S.nstep) return;
+    const int tid = threadIdx.x;
+    const bool act = tid < G::NTILES;
+    int I = 0, J = 0;
+    tile_of(act ? tid : 0, I, J);
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d4 = -d1 / 16.0;
+    double a[T][T];
+    if (act) {
+        w_tile<T>(S, S.vlt, tid, I, J, 2 * k - 1, 0.0, false, a);
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) {
+                const int i = I * T + r, j = J * T + c;
+                a[r][c] = (i == j) ? (i < S.n ? 0.125 : 0.0) : d4 * a[r][c];
+            }
+    } else {
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) a[r][c] = 0.0;
+    }
+    int bad = SWEEP_OK;
+    const int cnt = sweep_invert<T, NT>(a, vb, S.n, I, J, act, bad);
+    if (bad != SWEEP_OK) {
+        if (tid == 0) {
+            atomicMax(&S.prep[1], bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE);
+            atomicMin(&S.prep[2], k);
+        }
+        return;
+    }
+    if (tid == 0 && cnt) atomicAdd(&S.prep[0], cnt);
+    if (act) {
+        double *q = S.q + (size_t)(k - 1) * G::TT * S.ntiles + tid;
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) {
+                const int i = I * T + r, j = J * T + c;
+                // a = -U^{-1};  2HQ(C) = U^{-1} - 8I
+                const double x = (i == j && i < S.n) ? (-a[r][c] - 8.0) : -a[r][c];
+                q[(size_t)(r * T + c) * S.ntiles] = x;
+            }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MDPROP step loop, one CTA per job.  Dynamic shared memory: two 2HQ(C)
+// tile buffers filled by TMA bulk copies one step ahead, then (vl_smem) the
+// system's VL tiles.
+// ---------------------------------------------------------------------------
+template <int T, int NT>
+__global__ void __launch_bounds__(Geom<T, NT>::NTHR, Geom<T, NT>::MINB)
+ldmd_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs,
+                 double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                 int *__restrict__ kfail_out, int vl_smem)
+{
+    using G = Geom<T, NT>;
+    constexpr int NPAD = G::NPAD;
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ __align__(16) double vb[2 * G::VS];
+    __shared__ double s_y14[2][NPAD], s_y14b[2][NPAD], s_y23[2][NPAD];
+    __shared__ __align__(8) uint64_t qbar[2];
+    __shared__ SysDev s_sys;
+    const JobDev job = jobs[blockIdx.x];
+    if (threadIdx.x == 0) s_sys = systems[job.sys];
+    __syncthreads();
+    const SysDev &S = s_sys;
+    const int tid = threadIdx.x;
+    const bool act = tid < G::NTILES;
+    int I = 0, J = 0;
+    tile_of(act ? tid : 0, I, J);
+    const int n = S.n;
+    const int nt = S.ntiles;
+    const double ered = job.ered;
+    const size_t qdoubles = (size_t)G::TT * nt;
+    const uint32_t qbytes = (uint32_t)(qdoubles * sizeof(double));
+    double *qbuf0 = dsm;
+    double *vls = vl_smem ? dsm + 2 * qdoubles : nullptr;
+    const double *vl = vl_smem ? vls : S.vlt;
+
+    const int prep_status = S.prep[1];
+    if (prep_status != 0) {
+        if (tid == 0) {
+            status_out[job.out] = prep_status;
+            kfail_out[job.out] = S.prep[2];
+            nodes_out[job.out] = 0;
+        }
+        return;
+    }
+    if (tid == 0) {
+        mbar_init(&qbar[0], 1);
+        mbar_init(&qbar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < NPAD; i += G::NTHR) {
+        s_y14[0][i] = s_y14[1][i] = 0.0;
+        s_y14b[0][i] = s_y14b[1][i] = 0.0;
+        s_y23[0][i] = s_y23[1][i] = 0.0;
+    }
+    if (vl_smem) stage_vl(S, vls, G::TT, G::NTHR);
+    __syncthreads();
+    if (tid == 0) bulk_load(qbuf0 + qdoubles, S.q, qbytes, &qbar[1]);  // 2HQ(C_1) -> buffer 1
+
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d2 = 2.0 * d1;
+    const double half = 0.5 * h;
+    double *yj = y + job.yoff;
+
+    double a[T][T];
+    if (act) {
+        double w[T][T];
+        load_lower<T>(yj, n, I, J, a);
+        w_tile<T>(S, vl, tid, I, J, 0, ered, true, w);
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) a[r][c] = h * a[r][c] + d1 * w[r][c];  // mdprop.f:89-93
+    } else {
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) a[r][c] = 0.0;
+    }
+
+    int nodes = 0;
+    int status = MGPU_OK, kfail = 0;
+    int issued = 1;    // last step whose 2HQ(C) copy has been started
+    int consumed = 0;  // last step whose copy has been waited for
+    for (int k = 1; k <= S.nstep; ++k) {
+        const int sb = k & 1;
+        if (tid == 0 && k + 1 <= S.nstep) {
+            // buffer (k+1)&1 was last read in step k-1; every thread has passed
+            // that step's barriers, so the async proxy may overwrite it now
+            fence_async_shared();
+            bulk_load(qbuf0 + ((k + 1) & 1) * qdoubles, S.q + (size_t)k * qdoubles, qbytes, &qbar[(k + 1) & 1]);
+            issued = k + 1;
+        }
+        // reference-potential solutions in the sector (mdprop.f:143-164)
+        for (int i = tid; i < n; i += G::NTHR) {
+            const double wref = w_diag<T>(S, vl, i, 2 * k - 1, ered);
+            double y14, y23;
+            ref_solutions(wref, half, y14, y23);
+            s_y14[sb][i] = y14;
+            s_y14b[sb][i] = y14 - d1 * wref;
+            s_y23[sb][i] = y23;
+        }
+        __syncthreads();
+        if (act && I == J) {
+#pragma unroll
+            for (int r = 0; r < T; ++r) a[r][r] += s_y14b[sb][I * T + r];
+        }
+        int bad = SWEEP_OK;
+        nodes += sweep_invert<T, NT>(a, vb, n, I, J, act, bad);
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        // 2HQ(C_k) has landed in buffer k&1?  (bounded wait, uniform verdict)
+        const bool landed = mbar_wait_bounded(&qbar[sb], ((k - 1) >> 1) & 1);
+        if (__syncthreads_or(!landed)) {
+            status = MGPU_ERR_TIMEOUT;
+            kfail = k;
+            break;
+        }
+        consumed = k;
+        const double *qs = qbuf0 + sb * qdoubles + tid;
+        double y23r[T], y23c[T];
+#pragma unroll
+        for (int r = 0; r < T; ++r) y23r[r] = s_y23[sb][I * T + r];
+#pragma unroll
+        for (int c = 0; c < T; ++c) y23c[c] = s_y23[sb][J * T + c];
+        if (act) {
+            // Y = 2HQ(C) + 2 Y14 - Y23 Y^-1 Y23   (a holds -Y^-1), mdprop.f:156,181-185
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) a[r][c] = qs[(size_t)(r * T + c) * nt] + y23r[r] * a[r][c] * y23c[c];
+            if (I == J) {
+#pragma unroll
+                for (int r = 0; r < T; ++r) a[r][r] += 2.0 * s_y14[sb][I * T + r];
+            }
+        }
+        nodes += sweep_invert<T, NT>(a, vb, n, I, J, act, bad);
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        if (act) {
+            // Y = D2 W(B) - Y23 Y^-1 Y23 + Y14'   (mdprop.f:196-230)
+            const double dd = (k == S.nstep) ? d1 : d2;
+            double w[T][T];
+            w_tile<T>(S, vl, tid, I, J, 2 * k, ered, true, w);
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) a[r][c] = dd * w[r][c] + y23r[r] * a[r][c] * y23c[c];
+            if (I == J) {
+#pragma unroll
+                for (int r = 0; r < T; ++r) a[r][r] += s_y14b[sb][I * T + r];
+            }
+        }
+    }
+    if (status != MGPU_OK && tid == 0) {
+        // an early exit can leave up to two copies in flight: let them land
+        // (bounded) before this CTA's shared memory can be reused
+        for (int s2 = consumed + 1; s2 <= issued; ++s2) mbar_wait_bounded(&qbar[s2 & 1], ((s2 - 1) >> 1) & 1);
+    }
+    if (status == MGPU_OK && act) store_full<T>(yj, n, I, J, 1.0 / h, a);
+    if (tid == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes - S.prep[0] : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LDPROP step loop, one CTA per job (ldprop.f:46-147).  U(C) and Z are
+// inverted together; they are independent.
+// ---------------------------------------------------------------------------
+template <int T, int NT>
+__global__ void __launch_bounds__(Geom<T, NT>::NTHR, Geom<T, NT>::MINB)
+ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs,
+                double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                int *__restrict__ kfail_out, int vl_smem)
+{
+    using G = Geom<T, NT>;
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ __align__(16) double vz[2 * G::VS];
+    __shared__ __align__(16) double vu[2 * G::VS];
+    __shared__ SysDev s_sys;
+    const JobDev job = jobs[blockIdx.x];
+    if (threadIdx.x == 0) s_sys = systems[job.sys];
+    __syncthreads();
+    const SysDev &S = s_sys;
+    const int tid = threadIdx.x;
+    const bool act = tid < G::NTILES;
+    int I = 0, J = 0;
+    tile_of(act ? tid : 0, I, J);
+    const int n = S.n;
+    const double ered = job.ered;
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d2 = 2.0 * d1;
+    const double d4 = -d1 / 16.0;
+    double *yj = y + job.yoff;
+    if (vl_smem) stage_vl(S, dsm, G::TT, G::NTHR);
+    __syncthreads();
+    const double *vl = vl_smem ? dsm : S.vlt;
+
+    double z[T][T], u[T][T];
+#pragma unroll
+    for (int r = 0; r < T; ++r)
+#pragma unroll
+        for (int c = 0; c < T; ++c) { z[r][c] = 0.0; u[r][c] = 0.0; }
+    if (act) {
+        load_lower<T>(yj, n, I, J, z);
+        w_tile<T>(S, vl, tid, I, J, 0, ered, true, u);
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) {
+                const int i = I * T + r, j = J * T + c;
+                z[r][c] = h * z[r][c] + d1 * u[r][c] + ((i == j && i < n) ? 1.0 : 0.0);  // ldprop.f:46-51
+            }
+    }
+    int nodes = 0, status = MGPU_OK, kfail = 0;
+    for (int k = 1; k <= S.nstep; ++k) {
+        if (act) {
+            w_tile<T>(S, vl, tid, I, J, 2 * k - 1, ered, true, u);
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) {
+                    const int i = I * T + r, j = J * T + c;
+                    u[r][c] = d4 * u[r][c] + ((i == j && i < n) ? 0.125 : 0.0);  // ldprop.f:67-72
+                }
+        }
+        int bad = SWEEP_OK, ncz = 0;
+        const int ncu = sweep_invert2<T, NT>(u, z, vu, vz, n, I, J, act, ncz, bad);  // ldprop.f:78,83
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        nodes += ncz;
+        if (act) {
+            // Z = U^-1 - Z^-1 - 6I with u = -U^-1, z = -Z^-1 (ldprop.f:92-97)
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) {
+                    const int i = I * T + r, j = J * T + c;
+                    z[r][c] = -u[r][c] + z[r][c] - ((i == j && i < n) ? 6.0 : 0.0);
+                }
+        }
+        const int ncz2 = sweep_invert<T, NT>(z, vz, n, I, J, act, bad);  // ldprop.f:99
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        nodes += ncz2 - ncu;
+        if (act) {
+            const double dd = (k == S.nstep) ? d1 : d2;
+            w_tile<T>(S, vl, tid, I, J, 2 * k, ered, true, u);
+#pragma unroll
+            for (int r = 0; r < T; ++r)
+#pragma unroll
+                for (int c = 0; c < T; ++c) {
+                    const int i = I * T + r, j = J * T + c;
+                    // Z = D2 W(B) + 2I - Z^-1 (ldprop.f:114-131)
+                    z[r][c] = dd * u[r][c] + ((i == j && i < n) ? 2.0 : 0.0) + z[r][c];
+                }
+        }
+    }
+    if (status == MGPU_OK && act) {
+        // Y = Z/H - I/H (ldprop.f:140-147)
+        const double hi = 1.0 / h;
+#pragma unroll
+        for (int r = 0; r < T; ++r)
+#pragma unroll
+            for (int c = 0; c < T; ++c) {
+                const int i = I * T + r, j = J * T + c;
+                z[r][c] = hi * z[r][c] - ((i == j) ? hi : 0.0);
+            }
+        store_full<T>(yj, n, I, J, 1.0, z);
+    }
+    if (tid == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes : 0;
+    }
+}
+
+__global__ void prep_reset_kernel(int *prep, int nsys)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nsys) {
+        prep[3 * s] = 0;
+        prep[3 * s + 1] = 0;
+        prep[3 * s + 2] = 0x7fffffff;
+    }
+}
+
+// FP64 FMA pipe probe: 8 independent dependent-chains per thread.
+__global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int iters)
+{
+    double x[8];
+    const double s = 1.0 + 1e-9 * threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = 0.5 + 0.01 * i + 1e-7 * blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) x[i] = fma(x[i], s, -0.25);
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc += x[i];
+    if (acc == 12345.678) out[0] = acc;  // practically never true; keeps the chains live
+}
+
+// ---------------------------------------------------------------------------
+// bucket dispatch
+// ---------------------------------------------------------------------------
+#define MGPU_BUCKETS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(12) X(14) X(16)
+
+static const int kBucketNT[] = {
+#define X(nt) nt,
+    MGPU_BUCKETS(X)
+#undef X
+};
+static const int kNumBuckets = sizeof(kBucketNT) / sizeof(kBucketNT[0]);
+
+static int bucket_for(int n)
+{
+    for (int b = 0; b < kNumBuckets; ++b)
+        if (kT * kBucketNT[b] >= n) return b;
+    return -1;
+}
+
+static int ntiles_of(int b) { return kBucketNT[b] * (kBucketNT[b] + 1) / 2; }
+static int nthr_of(int b) { return ((ntiles_of(b) + 31) / 32) * 32; }
+
+static cudaError_t launch_prep(int b, dim3 grid, cudaStream_t st, const SysDev *sys, const int *list)
+{
+    switch (kBucketNT[b]) {
+#define X(nt)                                                                                  \
+    case nt:                                                                                   \
+        ldmd_prep_kernel<kT, nt><<<grid, Geom<kT, nt>::NTHR, 0, st>>>(sys, list);              \
+        break;
+        MGPU_BUCKETS(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class K>
+static cudaError_t set_smem(K kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+static cudaError_t launch_prop(int iprop, int b, int nblocks, size_t smem, int vl_smem, cudaStream_t st,
+                               const SysDev *sys, const JobDev *jobs, double *y, int *nodes, int *status, int *kfail)
+{
+    cudaError_t e = cudaSuccess;
+    switch (kBucketNT[b]) {
+#define X(nt)                                                                                                \
+    case nt:                                                                                                 \
+        if (iprop == MGPU_PROP_LDMD) {                                                                       \
+            if ((e = set_smem(ldmd_prop_kernel<kT, nt>, smem))) return e;                                    \
+            ldmd_prop_kernel<kT, nt><<<nblocks, Geom<kT, nt>::NTHR, smem, st>>>(sys, jobs, y, nodes, status, \
+                                                                                kfail, vl_smem);             \
+        } else {                                                                                             \
+            if ((e = set_smem(ldj_prop_kernel<kT, nt>, smem))) return e;                                     \
+            ldj_prop_kernel<kT, nt><<<nblocks, Geom<kT, nt>::NTHR, smem, st>>>(sys, jobs, y, nodes, status,  \
+                                                                               kfail, vl_smem);              \
+        }                                                                                                    \
+        break;
+        MGPU_BUCKETS(X)
+#undef X
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace mgpu
+
+// ===========================================================================
+// host side
+// ===========================================================================
+using namespace mgpu;
+
+static thread_local std::string g_last_error;
+
+static int set_err(int code, const char *what, cudaError_t e = cudaSuccess)
+{
+    char buf[512];
+    if (e != cudaSuccess)
+        snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+    else
+        snprintf(buf, sizeof buf, "%s", what);
+    g_last_error = buf;
+    return code;
+}
+
+struct mgpu_plan {
+    int iprop = 0;
+    int nsys = 0, njobs = 0;
+    std::vector<int> sys_n, sys_bucket, sys_nstep, sys_nham;
+    std::vector<size_t> yoff;      // per job, caller order
+    size_t yelems = 0;
+    double flops = 0.0;       // 3N^3 + 2 NHAM N(N+1) per job step (the reference's count)
+    double flops_prop = 0.0;  // what the propagation kernels do: (2|3)N^3 + 2 NHAM N(N+1) per job step
+    double flops_prep = 0.0;  // LDMD preparation: N^3 + NHAM N(N+1) per system step
+    // device memory
+    std::vector<void *> allocs;
+    SysDev *d_sys = nullptr;
+    JobDev *d_jobs = nullptr;
+    int *d_syslists = nullptr;
+    int *d_prep = nullptr;
+    // per bucket ranges (jobs sorted by bucket, systems listed by bucket)
+    std::vector<int> bucket_ids, job_begin, job_count, sys_begin, sys_count, max_nstep, vl_smem;
+    std::vector<size_t> smem;
+    // host staging for run_host
+    double *d_y = nullptr;
+    int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
+    size_t y_cap = 0;
+    int out_cap = 0;
+
+    ~mgpu_plan()
+    {
+        for (void *p : allocs) cudaFree(p);
+        if (d_y) cudaFree(d_y);
+        if (d_nodes) cudaFree(d_nodes);
+        if (d_status) cudaFree(d_status);
+        if (d_kfail) cudaFree(d_kfail);
+    }
+    template <class X>
+    cudaError_t dalloc(X **p, size_t count)
+    {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(X));
+        if (e == cudaSuccess) allocs.push_back(q);
+        *p = (X *)q;
+        return e;
+    }
+};
+
+template <class X>
+static cudaError_t upload(mgpu_plan *p, X **dst, const X *src, size_t count)
+{
+    cudaError_t e = p->dalloc(dst, count);
+    if (e != cudaSuccess) return e;
+    if (count) e = cudaMemcpy(*dst, src, count * sizeof(X), cudaMemcpyHostToDevice);
+    return e;
+}
+
+static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g)
+{
+    if (!c || !g) return set_err(MGPU_ERR_ARG, "null system or grid");
+    if (c->n < 1) return set_err(MGPU_ERR_ARG, "N must be >= 1");
+    if (c->nham < 0 || c->nvlblk < c->nham) return set_err(MGPU_ERR_ARG, "need 0 <= NHAM <= NVLBLK");
+    if (c->nham > 0 && !c->vl) return set_err(MGPU_ERR_ARG, "VL is null");
+    if (c->ivlfl > 0 && !c->iv) return set_err(MGPU_ERR_ARG, "IVLFL>0 but IV is null");
+    if (!c->eint || !c->cent) return set_err(MGPU_ERR_ARG, "EINT/CENT null");
+    if (g->nstep < 1) return set_err(MGPU_ERR_ARG, "NSTEP must be >= 1");
+    if (!g->rtab || (c->nham > 0 && !g->ptab)) return set_err(MGPU_ERR_ARG, "radial tables null");
+    if (!(g->dr != 0.0) || !std::isfinite(g->dr)) return set_err(MGPU_ERR_ARG, "DR must be finite and non-zero");
+    if (bucket_for(c->n) < 0) return set_err(MGPU_ERR_UNSUPPORTED, "N above the largest compiled bucket");
+    return MGPU_OK;
+}
+
+extern "C" {
+
+int mgpu_max_n(void) { return kT * kBucketNT[kNumBuckets - 1]; }
+
+int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out)
+{
+    if (!out_dev || iters < 1) return set_err(MGPU_ERR_ARG, "probe arguments");
+    int dev = 0, sms = 0, perSM = 0;
+    cudaError_t e;
+    if ((e = cudaGetDevice(&dev)) || (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)))
+        return set_err(MGPU_ERR_CUDA, "probe device query", e);
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, fp64_fma_probe_kernel, 256, 0)))
+        return set_err(MGPU_ERR_CUDA, "probe occupancy", e);
+    const int blocks = sms * std::max(perSM, 1);
+    fp64_fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(out_dev, iters);
+    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "probe launch", e);
+    if (flops_out) *flops_out = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)blocks;
+    return MGPU_OK;
+}
+
+const char *mgpu_last_error(void) { return g_last_error.c_str(); }
+
+const char *mgpu_status_string(int s)
+{
+    switch (s) {
+    case MGPU_OK: return "ok";
+    case MGPU_ERR_INVERSION: return "matrix inversion error (zero pivot)";
+    case MGPU_ERR_NONFINITE: return "non-finite pivot";
+    case MGPU_ERR_ARG: return "invalid argument";
+    case MGPU_ERR_CUDA: return "CUDA error";
+    case MGPU_ERR_UNSUPPORTED: return "unsupported size";
+    case MGPU_ERR_NOMEM: return "device allocation failed";
+    case MGPU_ERR_TIMEOUT: return "bounded wait for an asynchronous copy expired";
+    default: return "unknown status";
+    }
+}
+
+void mgpu_plan_destroy(mgpu_plan *plan) { delete plan; }
+
+size_t mgpu_plan_y_elems(const mgpu_plan *p) { return p ? p->yelems : 0; }
+
+size_t mgpu_plan_y_offset(const mgpu_plan *p, int job)
+{
+    return (p && job >= 0 && job < p->njobs) ? p->yoff[job] : 0;
+}
+
+double mgpu_plan_flops(const mgpu_plan *p) { return p ? p->flops : 0.0; }
+
+double mgpu_plan_flops_phase(const mgpu_plan *p, int phases)
+{
+    if (!p) return 0.0;
+    return ((phases & 1) ? p->flops_prep : 0.0) + ((phases & 2) ? p->flops_prop : 0.0);
+}
+
+int mgpu_plan_launches(const mgpu_plan *p)
+{
+    if (!p) return 0;
+    int l = (p->iprop == MGPU_PROP_LDMD) ? 1 : 0;  // prep_reset_kernel
+    for (size_t b = 0; b < p->bucket_ids.size(); ++b) {
+        if (p->iprop == MGPU_PROP_LDMD && p->sys_count[b] > 0) l += (p->sys_count[b] + 65534) / 65535;
+        if (p->job_count[b] > 0) ++l;
+    }
+    return l;
+}
+
+int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *systems,
+                     const mgpu_grid *grids, int njobs, const int *job_sys, const double *job_ered)
+{
+    if (!out) return set_err(MGPU_ERR_ARG, "null plan pointer");
+    *out = nullptr;
+    if (iprop != MGPU_PROP_LDMD && iprop != MGPU_PROP_LDJ) return set_err(MGPU_ERR_ARG, "IPROP must be 5 or 6");
+    if (nsys < 1 || njobs < 0 || !systems || !grids || (njobs > 0 && (!job_sys || !job_ered)))
+        return set_err(MGPU_ERR_ARG, "bad system/job arrays");
+    for (int s = 0; s < nsys; ++s) {
+        int rc = check_coupling(&systems[s], &grids[s]);
+        if (rc) return rc;
+    }
+    for (int j = 0; j < njobs; ++j)
+        if (job_sys[j] < 0 || job_sys[j] >= nsys || !std::isfinite(job_ered[j]))
+            return set_err(MGPU_ERR_ARG, "job references a bad system or ERED");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_err(MGPU_ERR_CUDA, "no CUDA device", e);
+
+    mgpu_plan *p = new (std::nothrow) mgpu_plan();
+    if (!p) return set_err(MGPU_ERR_NOMEM, "host allocation failed");
+    p->iprop = iprop;
+    p->nsys = nsys;
+    p->njobs = njobs;
+
+    std::vector<SysDev> hs(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        const mgpu_coupling &c = systems[s];
+        const mgpu_grid &g = grids[s];
+        const int b = bucket_for(c.n);
+        const int NT = kBucketNT[b];
+        const int npad = kT * NT;
+        const int nt = ntiles_of(b);
+        const int TT = kT * kT;
+        p->sys_n.push_back(c.n);
+        p->sys_bucket.push_back(b);
+        p->sys_nstep.push_back(g.nstep);
+        p->sys_nham.push_back(c.nham);
+        // VL / IV into the tile layout [term][element][tile]
+        const size_t tsz = (size_t)std::max(c.nham, 1) * TT * nt;
+        std::vector<double> vlt(tsz, 0.0);
+        std::vector<int> ivt(c.ivlfl > 0 ? tsz : 1, 0);
+        for (int t = 0; t < nt; ++t) {
+            int I = 0;
+            while ((I + 1) * (I + 2) / 2 <= t) ++I;
+            const int J = t - I * (I + 1) / 2;
+            for (int r = 0; r < kT; ++r)
+                for (int cc = 0; cc < kT; ++cc) {
+                    const int i = I * kT + r, j = J * kT + cc;
+                    if (i >= c.n || j >= c.n) continue;
+                    const int lo = std::min(i, j), hi = std::max(i, j);
+                    // pair (row lo, column hi) of the packed upper triangle (sumlam.f:33-36,74-86)
+                    const size_t pair = (size_t)hi * (hi + 1) / 2 + lo;
+                    for (int l = 0; l < c.nham; ++l) {
+                        const size_t src = pair * c.nvlblk + l;
+                        const size_t dst = ((size_t)l * TT + r * kT + cc) * nt + t;
+                        vlt[dst] = c.vl[src];
+                        if (c.ivlfl > 0) {
+                            int ix = c.iv[src] - 1;
+                            if (ix < 0 || ix >= c.nham) {
+                                delete p;
+                                return set_err(MGPU_ERR_ARG, "IV index outside 1..NHAM");
+                            }
+                            ivt[dst] = ix;
+                        }
+                    }
+                }
+        }
+        std::vector<double> eint(npad, 0.0), cent(npad, 0.0);
+        std::copy(c.eint, c.eint + c.n, eint.begin());
+        std::copy(c.cent, c.cent + c.n, cent.begin());
+        SysDev &d = hs[s];
+        memset(&d, 0, sizeof d);
+        d.n = c.n;
+        d.nham = c.nham;
+        d.ivlfl = c.ivlfl;
+        d.nconst = c.nconst;
+        d.nrsq = c.nrsq;
+        d.nstep = g.nstep;
+        d.ntiles = nt;
+        d.conlen = c.conlen;
+        d.dr = g.dr;
+        const size_t nr = 2 * (size_t)g.nstep + 1;
+        double *dv = nullptr, *de = nullptr, *dc = nullptr, *drt = nullptr, *dpt = nullptr, *dq = nullptr;
+        int *di = nullptr;
+        std::vector<double> pt(std::max<size_t>(nr * c.nham, 1), 0.0);
+        if (c.nham > 0) std::copy(g.ptab, g.ptab + nr * c.nham, pt.begin());
+        if ((e = upload(p, &dv, vlt.data(), vlt.size())) || (e = upload(p, &di, ivt.data(), ivt.size())) ||
+            (e = upload(p, &de, eint.data(), eint.size())) || (e = upload(p, &dc, cent.data(), cent.size())) ||
+            (e = upload(p, &drt, g.rtab, nr)) || (e = upload(p, &dpt, pt.data(), pt.size()))) {
+            delete p;
+            return set_err(MGPU_ERR_NOMEM, "uploading a system", e);
+        }
+        if (iprop == MGPU_PROP_LDMD) {
+            if ((e = p->dalloc(&dq, (size_t)g.nstep * TT * nt))) {
+                delete p;
+                return set_err(MGPU_ERR_NOMEM, "allocating the 2HQ(C) table", e);
+            }
+        }
+        d.vlt = dv;
+        d.ivt = di;
+        d.eint = de;
+        d.cent = dc;
+        d.rtab = drt;
+        d.ptab = dpt;
+        d.q = dq;
+    }
+    if (iprop == MGPU_PROP_LDMD)
+        for (int s = 0; s < nsys; ++s) {
+            const double n = systems[s].n, nh = systems[s].nham;
+            p->flops_prep += (n * n * n + nh * n * (n + 1.0)) * grids[s].nstep;
+        }
+    if ((e = p->dalloc(&p->d_prep, (size_t)3 * nsys))) {
+        delete p;
+        return set_err(MGPU_ERR_NOMEM, "allocating prep counters", e);
+    }
+    for (int s = 0; s < nsys; ++s) hs[s].prep = p->d_prep + 3 * s;
+    if ((e = upload(p, &p->d_sys, hs.data(), hs.size()))) {
+        delete p;
+        return set_err(MGPU_ERR_NOMEM, "uploading system descriptors", e);
+    }
+
+    // jobs: caller-order Y offsets; device order sorted by bucket then system
+    p->yoff.resize(njobs);
+    size_t off = 0;
+    for (int j = 0; j < njobs; ++j) {
+        p->yoff[j] = off;
+        const double n = systems[job_sys[j]].n;
+        off += (size_t)n * (size_t)n;
+        const double nh = systems[job_sys[j]].nham;
+        const double ns = grids[job_sys[j]].nstep;
+        p->flops += (3.0 * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
+        p->flops_prop += ((iprop == MGPU_PROP_LDMD ? 2.0 : 3.0) * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
+    }
+    p->yelems = off;
+    std::vector<int> order(njobs);
+    for (int j = 0; j < njobs; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        const int ba = p->sys_bucket[job_sys[a]], bb = p->sys_bucket[job_sys[b]];
+        if (ba != bb) return ba > bb;  // largest matrices first
+        return job_sys[a] < job_sys[b];
+    });
+    std::vector<JobDev> hj(njobs);
+    for (int k = 0; k < njobs; ++k) {
+        const int j = order[k];
+        hj[k].sys = job_sys[j];
+        hj[k].out = j;
+        hj[k].ered = job_ered[j];
+        hj[k].yoff = (long long)p->yoff[j];
+    }
+    std::vector<int> syslist;
+    for (int b = kNumBuckets - 1; b >= 0; --b) {
+        int jb = -1, jc = 0;
+        for (int k = 0; k < njobs; ++k)
+            if (p->sys_bucket[hj[k].sys] == b) {
+                if (jb < 0) jb = k;
+                ++jc;
+            }
+        int sb = (int)syslist.size(), sc = 0, mx = 0, nhmax = 0;
+        for (int s = 0; s < nsys; ++s)
+            if (p->sys_bucket[s] == b) {
+                syslist.push_back(s);
+                ++sc;
+                mx = std::max(mx, p->sys_nstep[s]);
+                nhmax = std::max(nhmax, p->sys_nham[s]);
+            }
+        if (jc == 0 && sc == 0) continue;
+        p->bucket_ids.push_back(b);
+        p->job_begin.push_back(jb < 0 ? 0 : jb);
+        p->job_count.push_back(jc);
+        p->sys_begin.push_back(sb);
+        p->sys_count.push_back(sc);
+        p->max_nstep.push_back(mx);
+        // shared memory: LDMD keeps two 2HQ(C) tile buffers; both kernels stage
+        // the VL tiles when they fit in the budget
+        const size_t tile_bytes = (size_t)kT * kT * ntiles_of(b) * sizeof(double);
+        const size_t base = iprop == MGPU_PROP_LDMD ? 2 * tile_bytes : 0;
+        const size_t vlb = (size_t)nhmax * tile_bytes;
+        const int use_vl = (base + vlb <= kSmemBudget) ? 1 : 0;
+        p->vl_smem.push_back(use_vl);
+        p->smem.push_back(base + (use_vl ? vlb : 0));
+    }
+    if ((e = upload(p, &p->d_jobs, hj.data(), hj.size())) ||
+        (e = upload(p, &p->d_syslists, syslist.data(), syslist.size()))) {
+        delete p;
+        return set_err(MGPU_ERR_NOMEM, "uploading jobs", e);
+    }
+    *out = p;
+    return MGPU_OK;
+}
+
+int mgpu_plan_run_device(mgpu_plan *p, double *y_dev, int *nodes_dev, int *status_dev, int *kfail_dev,
+                         void *stream)
+{
+    return mgpu_plan_run_device_phases(p, y_dev, nodes_dev, status_dev, kfail_dev, stream, 3);
+}
+
+int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int *status_dev, int *kfail_dev,
+                                void *stream, int phases)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (p->njobs > 0 && (!y_dev || !nodes_dev || !status_dev || !kfail_dev))
+        return set_err(MGPU_ERR_ARG, "null device buffer");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e;
+    if (p->iprop == MGPU_PROP_LDMD && (phases & 1)) {
+        // reset NSAVE / status / kfail of every system
+        prep_reset_kernel<<<(p->nsys + 127) / 128, 128, 0, st>>>(p->d_prep, p->nsys);
+        if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching prep_reset_kernel", e);
+        for (size_t b = 0; b < p->bucket_ids.size(); ++b) {
+            if (p->sys_count[b] == 0) continue;
+            for (int s0 = 0; s0 < p->sys_count[b]; s0 += 65535) {
+                dim3 grid(p->max_nstep[b], std::min(65535, p->sys_count[b] - s0));
+                if ((e = launch_prep(p->bucket_ids[b], grid, st, p->d_sys, p->d_syslists + p->sys_begin[b] + s0)))
+                    return set_err(MGPU_ERR_CUDA, "launching ldmd_prep_kernel", e);
+            }
+        }
+    }
+    for (size_t b = 0; b < p->bucket_ids.size() && (phases & 2); ++b) {
+        if (p->job_count[b] == 0) continue;
+        if ((e = launch_prop(p->iprop, p->bucket_ids[b], p->job_count[b], p->smem[b], p->vl_smem[b], st, p->d_sys,
+                             p->d_jobs + p->job_begin[b], y_dev, nodes_dev, status_dev, kfail_dev)))
+            return set_err(MGPU_ERR_CUDA, "launching the propagation kernel", e);
+    }
+    return MGPU_OK;
+}
+
+int mgpu_plan_run_host(mgpu_plan *p, double *y, int *nodes, int *status, int *kfail)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (p->njobs == 0) return MGPU_OK;
+    if (!y || !nodes || !status || !kfail) return set_err(MGPU_ERR_ARG, "null host buffer");
+    cudaError_t e;
+    if (p->y_cap < p->yelems) {
+        if (p->d_y) cudaFree(p->d_y);
+        p->d_y = nullptr;
+        if ((e = cudaMalloc(&p->d_y, p->yelems * sizeof(double)))) return set_err(MGPU_ERR_NOMEM, "Y buffer", e);
+        p->y_cap = p->yelems;
+    }
+    if (p->out_cap < p->njobs) {
+        if (p->d_nodes) cudaFree(p->d_nodes);
+        if (p->d_status) cudaFree(p->d_status);
+        if (p->d_kfail) cudaFree(p->d_kfail);
+        p->d_nodes = p->d_status = p->d_kfail = nullptr;
+        if ((e = cudaMalloc(&p->d_nodes, p->njobs * sizeof(int))) ||
+            (e = cudaMalloc(&p->d_status, p->njobs * sizeof(int))) ||
+            (e = cudaMalloc(&p->d_kfail, p->njobs * sizeof(int))))
+            return set_err(MGPU_ERR_NOMEM, "output buffers", e);
+        p->out_cap = p->njobs;
+    }
+    if ((e = cudaMemcpy(p->d_y, y, p->yelems * sizeof(double), cudaMemcpyHostToDevice)))
+        return set_err(MGPU_ERR_CUDA, "copying Y to the device", e);
+    int rc = mgpu_plan_run_device(p, p->d_y, p->d_nodes, p->d_status, p->d_kfail, nullptr);
+    if (rc) return rc;
+    if ((e = cudaDeviceSynchronize())) return set_err(MGPU_ERR_CUDA, "propagation", e);
+    if ((e = cudaMemcpy(y, p->d_y, p->yelems * sizeof(double), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(nodes, p->d_nodes, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(status, p->d_status, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)))
+        return set_err(MGPU_ERR_CUDA, "copying results to the host", e);
+    return MGPU_OK;
+}
+
+static int single(int iprop, const mgpu_coupling *c, const mgpu_grid *g, double ered, double *y, int *nodes,
+                  int *kfail)
+{
+    if (!y || !nodes || !kfail) return set_err(MGPU_ERR_ARG, "null output pointer");
+    mgpu_plan *p = nullptr;
+    int sys = 0;
+    int rc = mgpu_plan_create(&p, iprop, 1, c, g, 1, &sys, &ered);
+    if (rc) return rc;
+    int status = 0;
+    rc = mgpu_plan_run_host(p, y, nodes, &status, kfail);
+    mgpu_plan_destroy(p);
+    if (rc) return rc;
+    return status;
+}
+
+int mgpu_mdprop(const mgpu_coupling *c, const mgpu_grid *g, double ered, double *y, int *nodes, int *kfail)
+{
+    return single(MGPU_PROP_LDMD, c, g, ered, y, nodes, kfail);
+}
+
+int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered, double *z, int *nodes, int *kfail)
+{
+    return single(MGPU_PROP_LDJ, c, g, ered, z, nodes, kfail);
+}
+
+}  // extern "C"

@@ -1,0 +1,289 @@
+"""Host-side mirror of the MOLSCAT propagator interface over libmolscat_gpu.
+
+``mdprop`` / ``ldprop`` take the arguments of MDPROP (source_code/mdprop.f:1-4)
+and LDPROP (source_code/ldprop.f:1-4) with the same meaning and return
+``(Y, NODES)``.  Where the reference would ``STOP`` (mdprop.f:282-288,
+ldprop.f:151-153) they raise :class:`PropagatorError` carrying the same
+message.  The potential enters as a callable ``potenl(r) -> P`` evaluated on
+the host at every radius the propagator visits, exactly the values HAMMAT
+would compute (hammat.f:37-83); :func:`hammat_pvec` does that processing for
+a POTENL-style function.
+
+:class:`Plan` is the batched form: many systems and many (system, ERED) jobs
+in one set of device launches, with the energy-independent MDPROP inverses
+shared by all jobs of a system.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Callable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import Coupling_C, Grid_C, MGPU_PROP_LDJ, MGPU_PROP_LDMD
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class PropagatorError(RuntimeError):
+    def __init__(self, msg: str, status: int = 0, step: int = 0):
+        super().__init__(msg)
+        self.status = status
+        self.step = step
+
+
+@dataclass
+class Coupling:
+    """The propagator inputs that do not depend on R: VL(NVLBLK, N(N+1)/2)
+    packed upper-by-columns, IV of the same shape (1-based P indices, used
+    when IVLFL>0), EINT(N), CENT(N) and the module-potential flags."""
+    n: int
+    nham: int
+    vl: np.ndarray
+    eint: np.ndarray
+    cent: np.ndarray
+    nvlblk: int = 0
+    iv: np.ndarray | None = None
+    ivlfl: int = 0
+    nconst: int = 0
+    nrsq: int = 0
+    conlen: float = 0.0
+
+    def __post_init__(self):
+        if self.nvlblk == 0:
+            self.nvlblk = self.nham
+        self.vl = np.ascontiguousarray(self.vl, dtype=np.float64).ravel()
+        self.eint = np.ascontiguousarray(self.eint, dtype=np.float64).ravel()
+        self.cent = np.ascontiguousarray(self.cent, dtype=np.float64).ravel()
+        npair = self.n * (self.n + 1) // 2
+        if self.vl.size < self.nvlblk * npair:
+            raise ValueError(f"VL needs NVLBLK*N(N+1)/2 = {self.nvlblk * npair} values, got {self.vl.size}")
+        if self.eint.size < self.n or self.cent.size < self.n:
+            raise ValueError("EINT and CENT need N values")
+        if self.ivlfl > 0:
+            if self.iv is None:
+                raise ValueError("IVLFL>0 needs IV")
+            self.iv = np.ascontiguousarray(self.iv, dtype=np.int32).ravel()
+        else:
+            self.iv = np.zeros(1, dtype=np.int32)
+
+    def c_struct(self) -> Coupling_C:
+        return Coupling_C(self.n, self.nham, self.nvlblk, self.ivlfl, self.nconst, self.nrsq,
+                          float(self.conlen), self.vl.ctypes.data_as(_dp), self.iv.ctypes.data_as(_ip),
+                          self.eint.ctypes.data_as(_dp), self.cent.ctypes.data_as(_dp))
+
+
+def radial_grid(rstart: float, dr: float, nstep: int) -> np.ndarray:
+    """Radii R_k, k=0..2*NSTEP, accumulated as R=R+H the way MDPROP/LDPROP
+    step (mdprop.f:69,117,203; ldprop.f:30,57,105)."""
+    h = dr / 2.0
+    r = np.empty(2 * nstep + 1)
+    x = float(rstart)
+    r[0] = x
+    for k in range(1, 2 * nstep + 1):
+        x = x + h
+        r[k] = x
+    return r
+
+
+@dataclass
+class Segment:
+    """One propagation segment: NSTEP, DR and the P table at every radius."""
+    nstep: int
+    dr: float
+    rtab: np.ndarray
+    ptab: np.ndarray
+
+    @classmethod
+    def build(cls, rstart: float, dr: float, nstep: int, potential: Callable[[float], np.ndarray],
+              nham: int) -> "Segment":
+        rtab = radial_grid(rstart, dr, nstep)
+        ptab = np.empty((rtab.size, max(nham, 1)))
+        for k, r in enumerate(rtab):
+            ptab[k, :nham] = potential(float(r))[:nham]
+        return cls(nstep, dr, rtab, ptab)
+
+    def __post_init__(self):
+        self.rtab = np.ascontiguousarray(self.rtab, dtype=np.float64)
+        self.ptab = np.ascontiguousarray(self.ptab, dtype=np.float64)
+        if self.rtab.shape[0] != 2 * self.nstep + 1 or self.ptab.shape[0] != 2 * self.nstep + 1:
+            raise ValueError("tables need 2*NSTEP+1 rows")
+
+    def c_struct(self) -> Grid_C:
+        return Grid_C(int(self.nstep), float(self.dr), self.rtab.ctypes.data_as(_dp),
+                      self.ptab.ctypes.data_as(_dp))
+
+
+def hammat_pvec(potenl: Callable[[float], Sequence[float]], r: float, mxlam: int, ep2ru: float,
+                cm2ru: float, rscale: float = 1.0, vconst: Sequence[float] = (), nrsq: int = 0) -> np.ndarray:
+    """The P vector SUMLAM multiplies into VL at radius R (hammat.f:37-83):
+    POTENL(R*RSCALE) clamped at +-1e60, VCONST/EP2CM appended, scaled by
+    EP2RU, then NRSQ copies of min(1/R^2, 1e16).  SCAPOT and PERTRB are the
+    default (identity) hooks."""
+    p = np.zeros(mxlam + len(vconst) + nrsq)
+    p[:mxlam] = np.asarray(potenl(r * rscale), dtype=np.float64)[:mxlam]
+    big = np.abs(p[:mxlam]) > 1.0e60
+    p[:mxlam][big] = np.sign(p[:mxlam][big]) * 1.0e60
+    ep2cm = ep2ru / cm2ru
+    for i, v in enumerate(vconst):
+        p[mxlam + i] = v / ep2cm
+    p[: mxlam + len(vconst)] *= ep2ru
+    if nrsq:
+        p[mxlam + len(vconst):] = min(1.0 / (r * r), 1.0e16)
+    return p
+
+
+def _raise_for(name: str, status: int, step: int):
+    if status == _lib.MGPU_ERR_INVERSION or status == _lib.MGPU_ERR_NONFINITE:
+        if name == "MDPROP":
+            msg = f" ***** MDPROP: MATRIX INVERSION ERROR AT STEP K = {step:6d}.  RUN HALTED."
+        else:
+            msg = " *** ERROR IN SYMINV CALLED FROM LDPROP - TERMINATING"
+        if status == _lib.MGPU_ERR_NONFINITE:
+            msg += " (non-finite pivot)"
+        raise PropagatorError(msg, status, step)
+    raise PropagatorError(f"{name}: {_lib.status_string(status)}: {_lib.last_error()}", status, step)
+
+
+def _single(name, iprop, coupling: Coupling, seg: Segment, ered: float, y0: np.ndarray):
+    L = _lib.load()
+    n = coupling.n
+    y = np.array(y0, dtype=np.float64, order="F", copy=True)
+    if y.shape != (n, n):
+        raise ValueError(f"Y must be {n}x{n}")
+    c = coupling.c_struct()
+    g = seg.c_struct()
+    nodes = ctypes.c_int(0)
+    kfail = ctypes.c_int(0)
+    fn = L.mgpu_mdprop if iprop == MGPU_PROP_LDMD else L.mgpu_ldprop
+    rc = fn(ctypes.byref(c), ctypes.byref(g), float(ered), y.ctypes.data_as(_dp),
+            ctypes.byref(nodes), ctypes.byref(kfail))
+    if rc != 0:
+        _raise_for(name, rc, kfail.value)
+    return y, nodes.value
+
+
+def _args_to_inputs(n, mxlam, nham, vl, iv, eint, cent, rstart, rstop, nstep, dr, potential, nvlblk, ivlfl,
+                    nconst, nrsq, conlen):
+    coupling = Coupling(n=n, nham=nham, vl=vl, eint=eint, cent=cent, nvlblk=nvlblk or nham, iv=iv,
+                        ivlfl=ivlfl, nconst=nconst, nrsq=nrsq, conlen=conlen)
+    seg = Segment.build(rstart, dr, nstep, potential, nham)
+    return coupling, seg
+
+
+def mdprop(n, mxlam, nham, y, vl, iv, eint, cent, rstart, rstop, nstep, dr, ered, *, potential,
+           nvlblk=0, ivlfl=0, nconst=0, nrsq=0, conlen=0.0):
+    """MDPROP (mdprop.f:1-289) on the GPU.  ``potential(r)`` returns the P
+    vector HAMMAT would hand to SUMLAM at R (see :func:`hammat_pvec`).
+    Returns (Y at RSTOP as an N x N array, NODES)."""
+    del mxlam, rstop  # implied by NHAM/NSTEP/DR exactly as in the reference
+    coupling, seg = _args_to_inputs(n, 0, nham, vl, iv, eint, cent, rstart, None, nstep, dr, potential, nvlblk,
+                                    ivlfl, nconst, nrsq, conlen)
+    return _single("MDPROP", MGPU_PROP_LDMD, coupling, seg, ered, y)
+
+
+def ldprop(n, mxlam, nham, z, vl, iv, eint, cent, rstart, rstop, nstep, dr, ered, *, potential,
+           nvlblk=0, ivlfl=0, nconst=0, nrsq=0, conlen=0.0):
+    """LDPROP (ldprop.f:1-154) on the GPU.  Returns (Y at RSTOP, NODES)."""
+    del mxlam, rstop
+    coupling, seg = _args_to_inputs(n, 0, nham, vl, iv, eint, cent, rstart, None, nstep, dr, potential, nvlblk,
+                                    ivlfl, nconst, nrsq, conlen)
+    return _single("LDPROP", MGPU_PROP_LDJ, coupling, seg, ered, z)
+
+
+def propagate(prop: str, coupling: Coupling, seg: Segment, ered: float, y0: np.ndarray):
+    """One propagation from prepared inputs: prop is "LDMD" or "LDJ"."""
+    if prop == "LDMD":
+        return _single("MDPROP", MGPU_PROP_LDMD, coupling, seg, ered, y0)
+    if prop == "LDJ":
+        return _single("LDPROP", MGPU_PROP_LDJ, coupling, seg, ered, y0)
+    raise ValueError(prop)
+
+
+@dataclass
+class Plan:
+    """Batched propagation: ``systems[s]`` with ``segments[s]``; job j
+    propagates system ``job_sys[j]`` at ``job_ered[j]``."""
+    prop: str
+    systems: list
+    segments: list
+    job_sys: np.ndarray
+    job_ered: np.ndarray
+    _handle: ctypes.c_void_p = field(default=None, repr=False)
+
+    def __post_init__(self):
+        L = _lib.load()
+        self.iprop = MGPU_PROP_LDMD if self.prop == "LDMD" else MGPU_PROP_LDJ
+        if self.prop not in ("LDMD", "LDJ"):
+            raise ValueError(self.prop)
+        self.job_sys = np.ascontiguousarray(self.job_sys, dtype=np.int32)
+        self.job_ered = np.ascontiguousarray(self.job_ered, dtype=np.float64)
+        ns = len(self.systems)
+        cs = (Coupling_C * ns)(*[c.c_struct() for c in self.systems])
+        gs = (Grid_C * ns)(*[g.c_struct() for g in self.segments])
+        h = ctypes.c_void_p()
+        rc = L.mgpu_plan_create(ctypes.byref(h), self.iprop, ns, cs, gs, len(self.job_sys),
+                                self.job_sys.ctypes.data_as(_ip), self.job_ered.ctypes.data_as(_dp))
+        if rc != 0:
+            raise PropagatorError(f"plan: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+        self._handle = h
+        self.y_elems = int(L.mgpu_plan_y_elems(h))
+        self.offsets = np.array([L.mgpu_plan_y_offset(h, j) for j in range(len(self.job_sys))], dtype=np.int64)
+        self.flops = float(L.mgpu_plan_flops(h))
+        self.launches = int(L.mgpu_plan_launches(h))
+        self.flops_prep = float(L.mgpu_plan_flops_phase(h, 1))
+        self.flops_prop = float(L.mgpu_plan_flops_phase(h, 2))
+
+    @property
+    def njobs(self) -> int:
+        return len(self.job_sys)
+
+    def pack(self, ys: Sequence[np.ndarray]) -> np.ndarray:
+        buf = np.empty(self.y_elems)
+        for j, y in enumerate(ys):
+            n = self.systems[self.job_sys[j]].n
+            buf[self.offsets[j]:self.offsets[j] + n * n] = np.asarray(y, dtype=np.float64).ravel(order="F")
+        return buf
+
+    def unpack(self, buf: np.ndarray, j: int) -> np.ndarray:
+        n = self.systems[self.job_sys[j]].n
+        return buf[self.offsets[j]:self.offsets[j] + n * n].reshape((n, n), order="F")
+
+    def run_host(self, ybuf: np.ndarray):
+        """Host buffers in and out.  Returns (Y buffer, NODES, status, kfail)."""
+        L = _lib.load()
+        y = np.ascontiguousarray(ybuf, dtype=np.float64).copy()
+        nj = self.njobs
+        nodes = np.zeros(nj, dtype=np.int32)
+        status = np.zeros(nj, dtype=np.int32)
+        kfail = np.zeros(nj, dtype=np.int32)
+        rc = L.mgpu_plan_run_host(self._handle, y.ctypes.data_as(_dp), nodes.ctypes.data_as(_ip),
+                                  status.ctypes.data_as(_ip), kfail.ctypes.data_as(_ip))
+        if rc != 0:
+            raise PropagatorError(f"run: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+        return y, nodes, status, kfail
+
+    def run_device(self, y_ptr: int, nodes_ptr: int, status_ptr: int, kfail_ptr: int, stream: int = 0,
+                   phases: int = 3):
+        """Device buffers (raw pointers, e.g. torch ``data_ptr()``), async on
+        ``stream``.  phases: 1 = LDMD preparation only, 2 = propagation only."""
+        L = _lib.load()
+        rc = L.mgpu_plan_run_device_phases(self._handle, ctypes.c_void_p(y_ptr), ctypes.c_void_p(nodes_ptr),
+                                           ctypes.c_void_p(status_ptr), ctypes.c_void_p(kfail_ptr),
+                                           ctypes.c_void_p(stream), int(phases))
+        if rc != 0:
+            raise PropagatorError(f"run: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+
+    def close(self):
+        if self._handle:
+            _lib.load().mgpu_plan_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
