@@ -137,6 +137,37 @@ double mgpu_plan_flops_phase(const mgpu_plan *plan, int phases);
  * checksum so the work cannot be optimised away. */
 int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out);
 
+/* ---- allocation-free variant ---------------------------------------------
+ * mgpu_mdprop_noalloc: MDPROP for njobs energies of one system that makes no
+ * device allocation at all.  It has no counterpart in the reference.
+ *
+ * It exists for callers that cannot allocate device memory, for instance a
+ * program whose device memory all comes from its own pool or a framework
+ * allocator, or one that must not call cudaMalloc/cudaFree inside a
+ * latency-critical loop because those calls can synchronise the device.
+ *
+ * Every pointer inside *c and *g and every array argument is a DEVICE pointer
+ * owned by the caller: y_dev holds njobs consecutive N*N column-major
+ * matrices (initial Y in, Y(RSTOP) out), ered_dev the njobs reduced
+ * energies, and nodes_dev/status_dev/kfail_dev get one value per job, with
+ * the meanings of mgpu_mdprop.  The work is queued on `stream` (a
+ * cudaStream_t passed as void*, NULL = legacy default stream) and the call
+ * returns without waiting.
+ *
+ * Instead of allocating, the library uses one fixed 64 MiB scratch array,
+ * reserved on every GPU that loads the library until the process exits.  A
+ * request that needs more (about 128*NSTEP*NT*(NT+1)/2 bytes for the per-step
+ * 2HQ(C) table, NT = ceil(N/4)) or more than 4096 jobs is rejected with
+ * MGPU_ERR_UNSUPPORTED.  All calls share that array and it keeps the last
+ * call's contents (each call rewrites what it reads and zeroes its counters),
+ * so calls that overlap on the GPU -- on different streams or from different
+ * host threads -- race with each other: serialise them.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * should be made before any stream capture. */
+int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, int njobs,
+                        const double *ered_dev, double *y_dev, int *nodes_dev,
+                        int *status_dev, int *kfail_dev, void *stream);
+
 /* ---- diagnostics --------------------------------------------------------- */
 const char *mgpu_status_string(int status);
 const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */

@@ -44,7 +44,7 @@ EXPORTS = (
     "mgpu_plan_create", "mgpu_plan_destroy", "mgpu_plan_y_elems", "mgpu_plan_y_offset",
     "mgpu_plan_flops", "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
     "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
-    "mgpu_status_string", "mgpu_last_error", "mgpu_max_n",
+    "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc",
 )
 
 _lib = None
@@ -81,6 +81,7 @@ def load(path: str | None = None):
     L.mgpu_plan_flops_phase.argtypes = [vp, ctypes.c_int]
     L.mgpu_plan_flops_phase.restype = ctypes.c_double
     L.mgpu_probe_fp64_fma.argtypes = [vp, ctypes.c_int, vp, _dp]
+    L.mgpu_mdprop_noalloc.argtypes = [pc, pg, ctypes.c_int, vp, vp, vp, vp, vp, vp]
     L.mgpu_status_string.argtypes = [ctypes.c_int]
     L.mgpu_status_string.restype = ctypes.c_char_p
     L.mgpu_last_error.argtypes = []

@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1081,3 +1082,197 @@ int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered, double 
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free LDMD entry point (mgpu_mdprop_noalloc).
+//
+// Some callers cannot allocate device memory: a host program whose device
+// memory all comes from its own pool or framework allocator, or one that
+// must not call cudaMalloc/cudaFree inside a time-critical loop because
+// those calls can synchronise the whole device.  For them this entry point
+// uses no memory beyond the caller's own input/output buffers and one
+// file-scope scratch array of fixed size, reserved on every GPU that loads
+// this library until the process exits.  The kernels are the same ones the
+// plan API launches.
+// ===========================================================================
+namespace mgpu {
+
+constexpr size_t kNoAllocScratchBytes = (size_t)64 << 20;  // 64 MiB per device
+constexpr int kNoAllocMaxJobs = 4096;
+constexpr int kNoAllocMaxDevices = 64;
+
+// Holds, for one call at a time: the system descriptor, the job list, the
+// NSAVE/status counters, padded EINT/CENT, VL (and IV) in tile layout, and
+// the 2HQ(C) table of every step.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchBytes / sizeof(double)];
+
+static double *g_noalloc_addr[kNoAllocMaxDevices];  // device address of the array, per device
+static std::mutex g_noalloc_mu;
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Builds everything the LDMD kernels read from the scratch: descriptor, jobs
+// (ERED from the caller's device array), zeroed counters, padded EINT/CENT,
+// and VL/IV converted to the tile layout.  Every element the kernels read is
+// written, so nothing from an earlier call survives into this one.
+__global__ void noalloc_setup_kernel(SysDev proto, SysDev *sys_out, JobDev *jobs, int njobs, const double *ered,
+                                     int *syslist, const double *vl, const int *iv, int nvlblk, const double *eint,
+                                     const double *cent, double *eint_p, double *cent_p, double *vlt, int *ivt,
+                                     int npad, int T)
+{
+    const int TT = T * T;
+    const int nt = proto.ntiles;
+    const size_t nvlt = (size_t)proto.nham * TT * nt;
+    const size_t total = nvlt > (size_t)njobs ? nvlt : (size_t)njobs;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t x = (size_t)blockIdx.x * blockDim.x + threadIdx.x; x < total || x < (size_t)npad; x += stride) {
+        if (x == 0) {
+            *sys_out = proto;
+            syslist[0] = 0;
+            proto.prep[0] = 0;
+            proto.prep[1] = 0;
+            proto.prep[2] = 0x7fffffff;
+        }
+        if (x < (size_t)njobs) {
+            JobDev j;
+            j.sys = 0;
+            j.out = (int)x;
+            j.ered = ered[x];
+            j.yoff = (long long)x * proto.n * proto.n;
+            jobs[x] = j;
+        }
+        if (x < (size_t)npad) {
+            eint_p[x] = x < (size_t)proto.n ? eint[x] : 0.0;
+            cent_p[x] = x < (size_t)proto.n ? cent[x] : 0.0;
+        }
+        if (x < nvlt) {
+            const int t = (int)(x % nt);
+            const int e = (int)((x / nt) % TT);
+            const int l = (int)(x / ((size_t)nt * TT));
+            int I = 0;
+            while ((I + 1) * (I + 2) / 2 <= t) ++I;
+            const int J = t - I * (I + 1) / 2;
+            const int i = I * T + e / T, j = J * T + e % T;
+            double v = 0.0;
+            int ix = 0;
+            if (i < proto.n && j < proto.n) {
+                const int lo = i < j ? i : j, hi = i < j ? j : i;
+                const size_t src = ((size_t)hi * (hi + 1) / 2 + lo) * nvlblk + l;
+                v = vl[src];
+                if (proto.ivlfl > 0) {
+                    ix = iv[src] - 1;
+                    if (ix < 0 || ix >= proto.nham) {  // bad index: make the prep pass report it
+                        ix = 0;
+                        v = __longlong_as_double(0x7ff8000000000000LL);
+                    }
+                }
+            }
+            vlt[x] = v;
+            if (proto.ivlfl > 0) ivt[x] = ix;
+        }
+    }
+}
+
+}  // namespace mgpu
+
+extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, int njobs, const double *ered_dev,
+                                   double *y_dev, int *nodes_dev, int *status_dev, int *kfail_dev, void *stream)
+{
+    using namespace mgpu;
+    if (!c || !g) return set_err(MGPU_ERR_ARG, "null system or grid");
+    if (c->n < 1 || c->nham < 0 || c->nvlblk < c->nham || g->nstep < 1 || !(g->dr != 0.0) || !std::isfinite(g->dr))
+        return set_err(MGPU_ERR_ARG, "bad N/NHAM/NVLBLK/NSTEP/DR");
+    if (njobs < 1 || njobs > kNoAllocMaxJobs) return set_err(MGPU_ERR_UNSUPPORTED, "njobs must be 1..4096");
+    if ((c->nham > 0 && (!c->vl || !g->ptab)) || (c->ivlfl > 0 && !c->iv) || !c->eint || !c->cent || !g->rtab ||
+        !ered_dev || !y_dev || !nodes_dev || !status_dev || !kfail_dev)
+        return set_err(MGPU_ERR_ARG, "null device pointer");
+    const int b = bucket_for(c->n);
+    if (b < 0) return set_err(MGPU_ERR_UNSUPPORTED, "N above the largest compiled bucket");
+    const int nt = ntiles_of(b);
+    const int npad = kT * kBucketNT[b];
+    const size_t tile = (size_t)kT * kT * nt;  // doubles per tiled matrix
+
+    // scratch layout
+    size_t off = 0;
+    const size_t o_sys = off;
+    off = align256(off + sizeof(SysDev));
+    const size_t o_jobs = off;
+    off = align256(off + sizeof(JobDev) * (size_t)njobs);
+    const size_t o_prep = off;
+    off = align256(off + 4 * sizeof(int));
+    const size_t o_eint = off;
+    off = align256(off + sizeof(double) * npad);
+    const size_t o_cent = off;
+    off = align256(off + sizeof(double) * npad);
+    const size_t o_vlt = off;
+    off = align256(off + sizeof(double) * tile * (size_t)std::max(c->nham, 1));
+    const size_t o_ivt = off;
+    if (c->ivlfl > 0) off = align256(off + sizeof(int) * tile * (size_t)c->nham);
+    const size_t o_q = off;
+    off = align256(off + sizeof(double) * tile * (size_t)g->nstep);
+    if (off > kNoAllocScratchBytes) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "mgpu_mdprop_noalloc needs %zu bytes of scratch; the fixed limit is %zu (64 MiB)",
+                 off, kNoAllocScratchBytes);
+        return set_err(MGPU_ERR_UNSUPPORTED, buf);
+    }
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_err(MGPU_ERR_CUDA, "no CUDA device", e);
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return set_err(MGPU_ERR_UNSUPPORTED, "device ordinal above 63");
+    char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            // once per device, with that device current: the array's device address
+            double *ptr = nullptr;
+            e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess) return set_err(MGPU_ERR_CUDA, "cudaGetSymbolAddress(scratch)", e);
+            g_noalloc_addr[dev] = ptr;
+        }
+        base = reinterpret_cast<char *>(g_noalloc_addr[dev]);
+    }
+
+    SysDev proto;
+    memset(&proto, 0, sizeof proto);
+    proto.n = c->n;
+    proto.nham = c->nham;
+    proto.ivlfl = c->ivlfl;
+    proto.nconst = c->nconst;
+    proto.nrsq = c->nrsq;
+    proto.nstep = g->nstep;
+    proto.ntiles = nt;
+    proto.conlen = c->conlen;
+    proto.dr = g->dr;
+    proto.vlt = reinterpret_cast<double *>(base + o_vlt);
+    proto.ivt = reinterpret_cast<int *>(base + o_ivt);
+    proto.eint = reinterpret_cast<double *>(base + o_eint);
+    proto.cent = reinterpret_cast<double *>(base + o_cent);
+    proto.rtab = g->rtab;
+    proto.ptab = g->ptab;
+    proto.q = reinterpret_cast<double *>(base + o_q);
+    proto.prep = reinterpret_cast<int *>(base + o_prep);
+    SysDev *d_sys = reinterpret_cast<SysDev *>(base + o_sys);
+    JobDev *d_jobs = reinterpret_cast<JobDev *>(base + o_jobs);
+    int *d_list = proto.prep + 3;
+
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t work = std::max(std::max(tile * (size_t)std::max(c->nham, 1), (size_t)njobs), (size_t)npad);
+    const int blocks = (int)std::min<size_t>((work + 255) / 256, 4096);
+    noalloc_setup_kernel<<<blocks, 256, 0, st>>>(proto, d_sys, d_jobs, njobs, ered_dev, d_list, c->vl, c->iv,
+                                                 c->nvlblk, c->eint, c->cent, const_cast<double *>(proto.eint),
+                                                 const_cast<double *>(proto.cent), const_cast<double *>(proto.vlt),
+                                                 const_cast<int *>(proto.ivt), npad, kT);
+    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching noalloc_setup_kernel", e);
+    if ((e = launch_prep(b, dim3(g->nstep, 1), st, d_sys, d_list)))
+        return set_err(MGPU_ERR_CUDA, "launching ldmd_prep_kernel", e);
+    const size_t tile_bytes = tile * sizeof(double);
+    const size_t vlb = (size_t)c->nham * tile_bytes;
+    const int use_vl = (2 * tile_bytes + vlb <= kSmemBudget) ? 1 : 0;
+    const size_t smem = 2 * tile_bytes + (use_vl ? vlb : 0);
+    if ((e = launch_prop(MGPU_PROP_LDMD, b, njobs, smem, use_vl, st, d_sys, d_jobs, y_dev, nodes_dev, status_dev,
+                         kfail_dev)))
+        return set_err(MGPU_ERR_CUDA, "launching ldmd_prop_kernel", e);
+    return MGPU_OK;
+}
