@@ -1,0 +1,519 @@
+// LDMD / LDJ kernels on DMMA fragments: one warp per matrix (N <= 40).
+// Included by propagator.cu after SysDev, JobDev, ref_solutions.
+//
+// Fragment layout (see warp_dmma.cuh): for every lower 8x8 tile t and lane l,
+// the two doubles of element (8I + (l>>2), 8J + 2(l&3) + s) are stored at
+// [t][l][s], so one warp reads or writes a tile as 512 contiguous bytes.
+// VL is stored [term][t][l][s]; the 2HQ(C) table [step][t][l][s].
+#pragma once
+#include "warp_dmma.cuh"
+
+namespace mgpu {
+namespace wf {
+
+constexpr int kWPB = 4;  // warps (matrices) per CTA
+
+// per-warp shared memory (doubles): panel, y14, y14', y23, two 2HQ(C) buffers
+template <int NT>
+struct WarpSmem {
+    static constexpr int PAN = G<NT>::WSM;
+    static constexpr int VEC = G<NT>::NPAD;
+    static constexpr int QD = G<NT>::NTL * 64;
+    static constexpr int DOUBLES = PAN + 3 * VEC + 2 * QD;
+    static constexpr size_t BYTES = (size_t)DOUBLES * 8;
+};
+
+// W(R) on this lane's fragment (HAMMAT + SUMLAM, hammat.f:85-113).
+template <int NT>
+__device__ __forceinline__ void w_frag(const SysDev &S, int lane, int ir, double ered, bool diag_terms,
+                                       double (&w)[G<NT>::NTL][2])
+{
+    constexpr int NTL = G<NT>::NTL;
+    const double *P = S.ptab + (size_t)ir * S.nham;
+#pragma unroll
+    for (int t = 0; t < NTL; ++t) w[t][0] = w[t][1] = 0.0;
+    for (int l = 0; l < S.nham; ++l) {
+        const double *v = S.vlt + (size_t)l * NTL * 64 + lane * 2;
+        if (S.ivlfl <= 0) {
+            const double pl = __ldg(P + l);
+#pragma unroll
+            for (int t = 0; t < NTL; ++t) {
+                const double2 x = __ldg(reinterpret_cast<const double2 *>(v + t * 64));
+                w[t][0] = fma(x.x, pl, w[t][0]);
+                w[t][1] = fma(x.y, pl, w[t][1]);
+            }
+        } else {
+            const int *iv = S.ivt + (size_t)l * NTL * 64 + lane * 2;
+#pragma unroll
+            for (int t = 0; t < NTL; ++t)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const double x = __ldg(v + t * 64 + s);
+                    if (x != 0.0) w[t][s] = fma(x, __ldg(P + __ldg(iv + t * 64 + s)), w[t][s]);
+                }
+        }
+    }
+    if (diag_terms) {
+        const double R = __ldg(S.rtab + ir);
+        const double rsq = fmin(1.0 / (R * R), 1.0e16);
+        double conf = 0.0;
+        if (S.conlen > 0.0) {
+            const double c2 = S.conlen * S.conlen;
+            conf = R * R / (c2 * c2);
+        }
+        const int r = lane >> 2, q = lane & 3;
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int i = 8 * I + r;
+                if (r == 2 * q + s && i < S.n) {
+                    double x = w[tix(I, I)][s];
+                    if (S.nrsq == 0) x += rsq * S.cent[i];
+                    if (S.nconst == 0) x += S.eint[i];
+                    if (S.conlen > 0.0) x += conf;
+                    w[tix(I, I)][s] = x - ered;
+                }
+            }
+    }
+}
+
+// a <- dd * W(R) + yr_I a yc_J (+ y14' on the diagonal), one tile at a time
+// so W never lives in registers as a whole (mdprop.f:196-230).
+template <int NT>
+__device__ __forceinline__ void apply_wb_frag(const SysDev &S, int lane, int ir, double ered, double dd,
+                                              const double (&yr)[NT], const double (&yc)[NT][2],
+                                              const double *__restrict__ s_y14b, double (&a)[G<NT>::NTL][2])
+{
+    constexpr int NTL = G<NT>::NTL;
+    const double *P = S.ptab + (size_t)ir * S.nham;
+    const double R = __ldg(S.rtab + ir);
+    const double rsq = fmin(1.0 / (R * R), 1.0e16);
+    double conf = 0.0;
+    if (S.conlen > 0.0) {
+        const double c2 = S.conlen * S.conlen;
+        conf = R * R / (c2 * c2);
+    }
+    const int r = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J) {
+            const int t = tix(I, J);
+            double w0 = 0.0, w1 = 0.0;
+            const double *v = S.vlt + (size_t)t * 64 + lane * 2;
+            if (S.ivlfl <= 0) {
+                for (int l = 0; l < S.nham; ++l) {
+                    const double2 x = __ldg(reinterpret_cast<const double2 *>(v + (size_t)l * NTL * 64));
+                    const double pl = __ldg(P + l);
+                    w0 = fma(x.x, pl, w0);
+                    w1 = fma(x.y, pl, w1);
+                }
+            } else {
+                const int *iv = S.ivt + (size_t)t * 64 + lane * 2;
+                for (int l = 0; l < S.nham; ++l) {
+                    const double x0 = __ldg(v + (size_t)l * NTL * 64), x1 = __ldg(v + (size_t)l * NTL * 64 + 1);
+                    if (x0 != 0.0) w0 = fma(x0, __ldg(P + __ldg(iv + (size_t)l * NTL * 64)), w0);
+                    if (x1 != 0.0) w1 = fma(x1, __ldg(P + __ldg(iv + (size_t)l * NTL * 64 + 1)), w1);
+                }
+            }
+            if (I == J) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const int i = 8 * I + r;
+                    if (r == 2 * q + s && i < S.n) {
+                        double x = s ? w1 : w0;
+                        if (S.nrsq == 0) x += rsq * S.cent[i];
+                        if (S.nconst == 0) x += S.eint[i];
+                        if (S.conlen > 0.0) x += conf;
+                        x -= ered;
+                        if (s) w1 = x; else w0 = x;
+                    }
+                }
+            }
+            a[t][0] = dd * w0 + yr[I] * a[t][0] * yc[J][0];
+            a[t][1] = dd * w1 + yr[I] * a[t][1] * yc[J][1];
+            if (I == J) {
+                if (r == 2 * q) a[t][0] += s_y14b[8 * I + r];
+                if (r == 2 * q + 1) a[t][1] += s_y14b[8 * I + r];
+            }
+        }
+}
+
+// W(R)_ii (the DIAG array of HAMMAT) for channel i.
+template <int NT>
+__device__ __forceinline__ double w_diag_frag(const SysDev &S, int i, int ir, double ered)
+{
+    constexpr int NTL = G<NT>::NTL;
+    const int I = i >> 3, r = i & 7;
+    const int lane = r * 4 + (r >> 1), s = r & 1;  // lane holding (r, r) of tile (I, I)
+    const size_t e = (size_t)tix(I, I) * 64 + lane * 2 + s;
+    const double *P = S.ptab + (size_t)ir * S.nham;
+    double x = 0.0;
+    for (int l = 0; l < S.nham; ++l) {
+        const double v = __ldg(S.vlt + (size_t)l * NTL * 64 + e);
+        if (S.ivlfl <= 0) x = fma(v, __ldg(P + l), x);
+        else if (v != 0.0) x = fma(v, __ldg(P + __ldg(S.ivt + (size_t)l * NTL * 64 + e)), x);
+    }
+    const double R = __ldg(S.rtab + ir);
+    const double rsq = fmin(1.0 / (R * R), 1.0e16);
+    if (S.nrsq == 0) x += rsq * S.cent[i];
+    if (S.nconst == 0) x += S.eint[i];
+    if (S.conlen > 0.0) {
+        const double c2 = S.conlen * S.conlen;
+        x += R * R / (c2 * c2);
+    }
+    return x - ered;
+}
+
+template <int NT>
+__device__ __forceinline__ void load_lower_frag(const double *__restrict__ y, int n, int lane,
+                                                double (&a)[G<NT>::NTL][2])
+{
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int i = frow(I, lane), j = fcol(J, lane, s);
+                const int lo = i < j ? i : j, hi = i < j ? j : i;
+                a[tix(I, J)][s] = (i < n && j < n) ? y[(size_t)lo * n + hi] : 0.0;
+            }
+}
+
+template <int NT>
+__device__ __forceinline__ void store_full_frag(double *__restrict__ y, int n, int lane, double scale,
+                                                const double (&a)[G<NT>::NTL][2])
+{
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int i = frow(I, lane), j = fcol(J, lane, s);
+                if (i < n && j <= i) {
+                    const double x = scale * a[tix(I, J)][s];
+                    y[(size_t)j * n + i] = x;
+                    y[(size_t)i * n + j] = x;
+                }
+            }
+}
+
+// ---------------------------------------------------------------------------
+// MDPROP energy-independent half on fragments: grid (ceil(NSTEP/kWPB), systems).
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(32 * kWPB)
+ldmd_prep_frag_kernel(const SysDev *__restrict__ systems, const int *__restrict__ sys_list)
+{
+    constexpr int NTL = G<NT>::NTL;
+    __shared__ __align__(16) double pans[kWPB][G<NT>::WSM];
+    __shared__ SysDev s_sys;
+    if (threadIdx.x == 0) s_sys = systems[sys_list[blockIdx.y]];
+    __syncthreads();
+    const SysDev &S = s_sys;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = blockIdx.x * kWPB + warp + 1;
+    if (k > S.nstep) return;  // whole warp
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d4 = -d1 / 16.0;
+    double a[NTL][2];
+    w_frag<NT>(S, lane, 2 * k - 1, 0.0, false, a);
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int i = frow(I, lane), j = fcol(J, lane, s);
+                a[tix(I, J)][s] = (i == j) ? (i < S.n ? 0.125 : 0.0) : d4 * a[tix(I, J)][s];
+            }
+    int bad = SWEEP_OK;
+    const int cnt = warp_sweep_invert<NT>(a, pans[warp], S.n, lane, bad);
+    if (bad != SWEEP_OK) {
+        if (lane == 0) {
+            atomicMax(&S.prep[1], bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE);
+            atomicMin(&S.prep[2], k);
+        }
+        return;
+    }
+    if (lane == 0 && cnt) atomicAdd(&S.prep[0], cnt);
+    double *q = S.q + (size_t)(k - 1) * NTL * 64 + lane * 2;
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J) {
+            double2 v;
+            const int i = frow(I, lane);
+            // a = -U^{-1};  2HQ(C) = U^{-1} - 8I
+            const int j0 = fcol(J, lane, 0), j1 = fcol(J, lane, 1);
+            v.x = (i >= S.n || j0 >= S.n) ? 0.0 : (i == j0 ? -a[tix(I, J)][0] - 8.0 : -a[tix(I, J)][0]);
+            v.y = (i >= S.n || j1 >= S.n) ? 0.0 : (i == j1 ? -a[tix(I, J)][1] - 8.0 : -a[tix(I, J)][1]);
+            *reinterpret_cast<double2 *>(q + tix(I, J) * 64) = v;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// MDPROP step loop, one warp per job.
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(32 * kWPB, 3)
+ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs,
+                      double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                      int *__restrict__ kfail_out)
+{
+    constexpr int NTL = G<NT>::NTL;
+    constexpr int NPAD = G<NT>::NPAD;
+    using W = WarpSmem<NT>;
+    extern __shared__ __align__(16) double dsm[];
+    __shared__ __align__(8) uint64_t qbar[kWPB][2];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int jix = blockIdx.x * kWPB + warp;
+    if (jix >= njobs) return;  // whole warp; the kernel has no CTA-wide barrier
+    const JobDev job = jobs[jix];
+    const SysDev &S = systems[job.sys];
+    double *pan = dsm + (size_t)warp * W::DOUBLES;
+    double *s_y14 = pan + W::PAN;
+    double *s_y14b = s_y14 + W::VEC;
+    double *s_y23 = s_y14b + W::VEC;
+    double *qbuf = s_y23 + W::VEC;
+    const int n = S.n;
+    const int nstep = S.nstep;
+    const double ered = job.ered;
+    const uint32_t qbytes = (uint32_t)(NTL * 64 * sizeof(double));
+    uint64_t *bar = qbar[warp];
+
+    if (S.prep[1] != 0) {
+        if (lane == 0) {
+            status_out[job.out] = S.prep[1];
+            kfail_out[job.out] = S.prep[2];
+            nodes_out[job.out] = 0;
+        }
+        return;
+    }
+    for (int i = lane; i < NPAD; i += 32) s_y14[i] = s_y14b[i] = s_y23[i] = 0.0;
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (lane == 0) bulk_load(qbuf + NTL * 64, S.q, qbytes, &bar[1]);  // 2HQ(C_1) -> buffer 1
+
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d2 = 2.0 * d1;
+    const double half = 0.5 * h;
+    double *yj = y + job.yoff;
+
+    double a[NTL][2];
+    {
+        double w[NTL][2];
+        load_lower_frag<NT>(yj, n, lane, a);
+        w_frag<NT>(S, lane, 0, ered, true, w);
+#pragma unroll
+        for (int t = 0; t < NTL; ++t)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) a[t][s] = h * a[t][s] + d1 * w[t][s];  // mdprop.f:89-93
+    }
+    const int r = lane >> 2, q = lane & 3;
+    int nodes = 0, status = MGPU_OK, kfail = 0;
+    int issued = 1, consumed = 0;
+    for (int k = 1; k <= nstep; ++k) {
+        const int sb = k & 1;
+        if (lane == 0 && k + 1 <= nstep) {
+            fence_async_shared();
+            bulk_load(qbuf + ((k + 1) & 1) * NTL * 64, S.q + (size_t)k * NTL * 64, qbytes, &bar[(k + 1) & 1]);
+            issued = k + 1;
+        }
+        // reference-potential solutions in the sector (mdprop.f:143-164)
+        __syncwarp();
+        for (int i = lane; i < n; i += 32) {
+            const double wref = w_diag_frag<NT>(S, i, 2 * k - 1, ered);
+            double y14, y23;
+            ref_solutions(wref, half, y14, y23);
+            s_y14[i] = y14;
+            s_y14b[i] = y14 - d1 * wref;
+            s_y23[i] = y23;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+                if (r == 2 * q + s) a[tix(I, I)][s] += s_y14b[8 * I + r];
+        int bad = SWEEP_OK;
+        nodes += warp_sweep_invert<NT>(a, pan, n, lane, bad);
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        const bool landed = mbar_wait_bounded(&bar[sb], ((k - 1) >> 1) & 1);
+        if (__any_sync(0xffffffffu, !landed)) {
+            status = MGPU_ERR_TIMEOUT;
+            kfail = k;
+            break;
+        }
+        consumed = k;
+        double yr[NT], yc[NT][2];
+#pragma unroll
+        for (int I = 0; I < NT; ++I) {
+            yr[I] = s_y23[8 * I + r];
+            yc[I][0] = s_y23[8 * I + 2 * q];
+            yc[I][1] = s_y23[8 * I + 2 * q + 1];
+        }
+        {
+            const double *qs = qbuf + sb * NTL * 64 + lane * 2;
+            // Y = 2HQ(C) + 2 Y14 - Y23 Y^-1 Y23   (a holds -Y^-1), mdprop.f:156,181-185
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int J = 0; J <= I; ++J) {
+                    const double2 qq = *reinterpret_cast<const double2 *>(qs + tix(I, J) * 64);
+                    a[tix(I, J)][0] = qq.x + yr[I] * a[tix(I, J)][0] * yc[J][0];
+                    a[tix(I, J)][1] = qq.y + yr[I] * a[tix(I, J)][1] * yc[J][1];
+                }
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    if (r == 2 * q + s) a[tix(I, I)][s] += 2.0 * s_y14[8 * I + r];
+        }
+        nodes += warp_sweep_invert<NT>(a, pan, n, lane, bad);
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        // Y = D2 W(B) - Y23 Y^-1 Y23 + Y14'   (mdprop.f:196-230)
+        apply_wb_frag<NT>(S, lane, 2 * k, ered, (k == nstep) ? d1 : d2, yr, yc, s_y14b, a);
+    }
+    if (status != MGPU_OK && lane == 0) {
+        for (int s2 = consumed + 1; s2 <= issued; ++s2) mbar_wait_bounded(&bar[s2 & 1], ((s2 - 1) >> 1) & 1);
+    }
+    __syncwarp();
+    if (status == MGPU_OK) store_full_frag<NT>(yj, n, lane, 1.0 / h, a);
+    if (lane == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes - S.prep[0] : 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// LDPROP step loop, one warp per job (ldprop.f:46-147).
+// ---------------------------------------------------------------------------
+template <int NT>
+__global__ void __launch_bounds__(32 * kWPB)
+ldj_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs,
+                     double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                     int *__restrict__ kfail_out)
+{
+    constexpr int NTL = G<NT>::NTL;
+    __shared__ __align__(16) double pans[kWPB][G<NT>::WSM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int jix = blockIdx.x * kWPB + warp;
+    if (jix >= njobs) return;
+    const JobDev job = jobs[jix];
+    const SysDev &S = systems[job.sys];
+    double *pan = pans[warp];
+    const int n = S.n;
+    const double ered = job.ered;
+    const double h = S.dr / 2.0;
+    const double d1 = h * h / 3.0;
+    const double d2 = 2.0 * d1;
+    const double d4 = -d1 / 16.0;
+    double *yj = y + job.yoff;
+    const int r = lane >> 2, q = lane & 3;
+
+    double z[NTL][2], u[NTL][2];
+    load_lower_frag<NT>(yj, n, lane, z);
+    w_frag<NT>(S, lane, 0, ered, true, u);
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int J = 0; J <= I; ++J)
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                z[tix(I, J)][s] = h * z[tix(I, J)][s] + d1 * u[tix(I, J)][s] + (dg ? 1.0 : 0.0);  // ldprop.f:46-51
+            }
+    int nodes = 0, status = MGPU_OK, kfail = 0;
+    for (int k = 1; k <= S.nstep; ++k) {
+        w_frag<NT>(S, lane, 2 * k - 1, ered, true, u);
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                    u[tix(I, J)][s] = d4 * u[tix(I, J)][s] + (dg ? 0.125 : 0.0);  // ldprop.f:67-72
+                }
+        int bad = SWEEP_OK;
+        const int ncu = warp_sweep_invert<NT>(u, pan, n, lane, bad);  // ldprop.f:78
+        int bad2 = SWEEP_OK;
+        const int ncz = warp_sweep_invert<NT>(z, pan, n, lane, bad2);  // ldprop.f:83
+        if (bad != SWEEP_OK || bad2 != SWEEP_OK) {
+            status = (bad == SWEEP_ZERO || bad2 == SWEEP_ZERO) ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        nodes += ncz;
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                    // Z = U^-1 - Z^-1 - 6I with u = -U^-1, z = -Z^-1 (ldprop.f:92-97)
+                    z[tix(I, J)][s] = -u[tix(I, J)][s] + z[tix(I, J)][s] - (dg ? 6.0 : 0.0);
+                }
+        const int ncz2 = warp_sweep_invert<NT>(z, pan, n, lane, bad);  // ldprop.f:99
+        if (bad != SWEEP_OK) {
+            status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+            kfail = k;
+            break;
+        }
+        nodes += ncz2 - ncu;
+        const double dd = (k == S.nstep) ? d1 : d2;
+        w_frag<NT>(S, lane, 2 * k, ered, true, u);
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                    // Z = D2 W(B) + 2I - Z^-1 (ldprop.f:114-131)
+                    z[tix(I, J)][s] = dd * u[tix(I, J)][s] + (dg ? 2.0 : 0.0) + z[tix(I, J)][s];
+                }
+    }
+    if (status == MGPU_OK) {
+        // Y = Z/H - I/H (ldprop.f:140-147)
+        const double hi = 1.0 / h;
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int J = 0; J <= I; ++J)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) {
+                    const bool dg = (I == J) && (r == 2 * q + s);
+                    z[tix(I, J)][s] = hi * z[tix(I, J)][s] - (dg ? hi : 0.0);
+                }
+        store_full_frag<NT>(yj, n, lane, 1.0, z);
+    }
+    if (lane == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes : 0;
+    }
+}
+
+}  // namespace wf
+}  // namespace mgpu

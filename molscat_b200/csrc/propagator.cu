@@ -32,7 +32,7 @@ constexpr int kT = 4;  // tile edge of every compiled bucket
 constexpr size_t kSmemBudget = 96 * 1024;  // dynamic shared memory per CTA we allow
 
 struct SysDev {
-    int n, nham, ivlfl, nconst, nrsq, nstep, ntiles, pad0;
+    int n, nham, ivlfl, nconst, nrsq, nstep, ntiles, kind;  // kind: 0 = 4x4 register tiles, 1 = 8x8 DMMA fragments
     double conlen, dr;
     const double *vlt;  // [nham][T*T][ntiles] tile layout, zero padding
     const int *ivt;     // same shape, 0-based P index (ivlfl > 0 only)
@@ -545,6 +545,10 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
     }
 }
 
+}  // namespace mgpu
+#include "kernels_frag.cuh"
+namespace mgpu {
+
 __global__ void prep_reset_kernel(int *prep, int nsys)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -578,36 +582,42 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int it
 // bucket dispatch
 // ---------------------------------------------------------------------------
 #define MGPU_BUCKETS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(12) X(14) X(16)
+#define MGPU_FRAG_BUCKETS(X) X(1) X(2) X(3) X(4) X(5)
 
-static const int kBucketNT[] = {
-#define X(nt) nt,
+enum { KIND_TILE4 = 0, KIND_FRAG8 = 1 };
+
+struct Bucket {
+    int kind;
+    int nt;
+};
+
+// 8x8-fragment buckets first (preferred for N <= 40), then 4x4 register tiles.
+static const Bucket kBuckets[] = {
+#define X(nt) {KIND_FRAG8, nt},
+    MGPU_FRAG_BUCKETS(X)
+#undef X
+#define X(nt) {KIND_TILE4, nt},
     MGPU_BUCKETS(X)
 #undef X
 };
-static const int kNumBuckets = sizeof(kBucketNT) / sizeof(kBucketNT[0]);
+static const int kNumBuckets = sizeof(kBuckets) / sizeof(kBuckets[0]);
 
+static int bucket_edge(int b) { return kBuckets[b].kind == KIND_FRAG8 ? 8 : kT; }
+static int bucket_npad(int b) { return bucket_edge(b) * kBuckets[b].nt; }
+static int ntiles_of(int b) { return kBuckets[b].nt * (kBuckets[b].nt + 1) / 2; }
+static size_t tile_elems(int b) { return (size_t)bucket_edge(b) * bucket_edge(b); }  // doubles per tile
+static size_t matrix_elems(int b) { return tile_elems(b) * ntiles_of(b); }         // doubles per tiled matrix
+
+// Smallest bucket of the preferred kind that holds N (falls back to the other kind).
+static int g_prefer_kind = KIND_FRAG8;
 static int bucket_for(int n)
 {
-    for (int b = 0; b < kNumBuckets; ++b)
-        if (kT * kBucketNT[b] >= n) return b;
-    return -1;
-}
-
-static int ntiles_of(int b) { return kBucketNT[b] * (kBucketNT[b] + 1) / 2; }
-static int nthr_of(int b) { return ((ntiles_of(b) + 31) / 32) * 32; }
-
-static cudaError_t launch_prep(int b, dim3 grid, cudaStream_t st, const SysDev *sys, const int *list)
-{
-    switch (kBucketNT[b]) {
-#define X(nt)                                                                                  \
-    case nt:                                                                                   \
-        ldmd_prep_kernel<kT, nt><<<grid, Geom<kT, nt>::NTHR, 0, st>>>(sys, list);              \
-        break;
-        MGPU_BUCKETS(X)
-#undef X
-    default: return cudaErrorInvalidValue;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int kind = pass == 0 ? g_prefer_kind : 1 - g_prefer_kind;
+        for (int b = 0; b < kNumBuckets; ++b)
+            if (kBuckets[b].kind == kind && bucket_npad(b) >= n) return b;
     }
-    return cudaGetLastError();
+    return -1;
 }
 
 template <class K>
@@ -617,28 +627,122 @@ static cudaError_t set_smem(K kernel, size_t bytes)
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-static cudaError_t launch_prop(int iprop, int b, int nblocks, size_t smem, int vl_smem, cudaStream_t st,
+// grid.x counts steps, grid.y systems
+static cudaError_t launch_prep(int b, int max_nstep, int nsys, cudaStream_t st, const SysDev *sys, const int *list)
+{
+    const int nt = kBuckets[b].nt;
+    if (kBuckets[b].kind == KIND_FRAG8) {
+        dim3 grid((max_nstep + wf::kWPB - 1) / wf::kWPB, nsys);
+        switch (nt) {
+#define X(t)                                                                          \
+    case t: wf::ldmd_prep_frag_kernel<t><<<grid, 32 * wf::kWPB, 0, st>>>(sys, list); \
+        break;
+            MGPU_FRAG_BUCKETS(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+        }
+    } else {
+        dim3 grid(max_nstep, nsys);
+        switch (nt) {
+#define X(t)                                                                                 \
+    case t: ldmd_prep_kernel<kT, t><<<grid, Geom<kT, t>::NTHR, 0, st>>>(sys, list); \
+        break;
+            MGPU_BUCKETS(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    return cudaGetLastError();
+}
+
+// Dynamic shared memory a propagation launch of bucket b needs (vl_smem: the
+// 4x4-tile kernels stage VL when it fits).
+static size_t prop_smem(int iprop, int b, int nham, int *vl_smem)
+{
+    if (kBuckets[b].kind == KIND_FRAG8) {
+        *vl_smem = 0;
+        size_t per = 0;
+        switch (kBuckets[b].nt) {
+#define X(t) case t: per = wf::WarpSmem<t>::BYTES; break;
+            MGPU_FRAG_BUCKETS(X)
+#undef X
+        }
+        return iprop == MGPU_PROP_LDMD ? per * wf::kWPB : 0;
+    }
+    const size_t tile_bytes = matrix_elems(b) * sizeof(double);
+    const size_t base = iprop == MGPU_PROP_LDMD ? 2 * tile_bytes : 0;
+    const size_t vlb = (size_t)nham * tile_bytes;
+    *vl_smem = (base + vlb <= kSmemBudget) ? 1 : 0;
+    return base + (*vl_smem ? vlb : 0);
+}
+
+static cudaError_t launch_prop(int iprop, int b, int njobs, size_t smem, int vl_smem, cudaStream_t st,
                                const SysDev *sys, const JobDev *jobs, double *y, int *nodes, int *status, int *kfail)
 {
     cudaError_t e = cudaSuccess;
-    switch (kBucketNT[b]) {
-#define X(nt)                                                                                                \
-    case nt:                                                                                                 \
-        if (iprop == MGPU_PROP_LDMD) {                                                                       \
-            if ((e = set_smem(ldmd_prop_kernel<kT, nt>, smem))) return e;                                    \
-            ldmd_prop_kernel<kT, nt><<<nblocks, Geom<kT, nt>::NTHR, smem, st>>>(sys, jobs, y, nodes, status, \
-                                                                                kfail, vl_smem);             \
-        } else {                                                                                             \
-            if ((e = set_smem(ldj_prop_kernel<kT, nt>, smem))) return e;                                     \
-            ldj_prop_kernel<kT, nt><<<nblocks, Geom<kT, nt>::NTHR, smem, st>>>(sys, jobs, y, nodes, status,  \
-                                                                               kfail, vl_smem);              \
-        }                                                                                                    \
+    const int nt = kBuckets[b].nt;
+    if (kBuckets[b].kind == KIND_FRAG8) {
+        const int blocks = (njobs + wf::kWPB - 1) / wf::kWPB;
+        switch (nt) {
+#define X(t)                                                                                                  \
+    case t:                                                                                                   \
+        if (iprop == MGPU_PROP_LDMD) {                                                                        \
+            if ((e = set_smem(wf::ldmd_prop_frag_kernel<t>, smem))) return e;                                 \
+            wf::ldmd_prop_frag_kernel<t><<<blocks, 32 * wf::kWPB, smem, st>>>(sys, jobs, njobs, y, nodes,     \
+                                                                              status, kfail);                 \
+        } else {                                                                                              \
+            wf::ldj_prop_frag_kernel<t><<<blocks, 32 * wf::kWPB, 0, st>>>(sys, jobs, njobs, y, nodes, status, \
+                                                                          kfail);                             \
+        }                                                                                                     \
+        break;
+            MGPU_FRAG_BUCKETS(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
+    switch (nt) {
+#define X(t)                                                                                                \
+    case t:                                                                                                 \
+        if (iprop == MGPU_PROP_LDMD) {                                                                      \
+            if ((e = set_smem(ldmd_prop_kernel<kT, t>, smem))) return e;                                    \
+            ldmd_prop_kernel<kT, t><<<njobs, Geom<kT, t>::NTHR, smem, st>>>(sys, jobs, y, nodes, status,    \
+                                                                           kfail, vl_smem);                 \
+        } else {                                                                                            \
+            if ((e = set_smem(ldj_prop_kernel<kT, t>, smem))) return e;                                     \
+            ldj_prop_kernel<kT, t><<<njobs, Geom<kT, t>::NTHR, smem, st>>>(sys, jobs, y, nodes, status,     \
+                                                                          kfail, vl_smem);                  \
+        }                                                                                                   \
         break;
         MGPU_BUCKETS(X)
 #undef X
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+// Element (i, j) of tile t, position e, for either layout.
+static void tile_element(int b, int t, int e, int *i, int *j)
+{
+    int I = 0;
+    while ((I + 1) * (I + 2) / 2 <= t) ++I;
+    const int J = t - I * (I + 1) / 2;
+    if (kBuckets[b].kind == KIND_FRAG8) {
+        const int lane = e >> 1, s = e & 1;
+        *i = 8 * I + (lane >> 2);
+        *j = 8 * J + 2 * (lane & 3) + s;
+    } else {
+        *i = kT * I + e / kT;
+        *j = kT * J + e % kT;
+    }
+}
+
+// Offset of (term l, tile t, position e) in the system's VL/IV/2HQ(C) arrays.
+static size_t tile_offset(int b, int l, int t, int e)
+{
+    const int nt = ntiles_of(b);
+    if (kBuckets[b].kind == KIND_FRAG8) return ((size_t)l * nt + t) * 64 + e;
+    return ((size_t)l * tile_elems(b) + e) * nt + t;
 }
 
 }  // namespace mgpu
@@ -730,7 +834,12 @@ static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g)
 
 extern "C" {
 
-int mgpu_max_n(void) { return kT * kBucketNT[kNumBuckets - 1]; }
+int mgpu_max_n(void)
+{
+    int m = 0;
+    for (int b = 0; b < kNumBuckets; ++b) m = std::max(m, bucket_npad(b));
+    return m;
+}
 
 int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out)
 {
@@ -823,44 +932,39 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         const mgpu_coupling &c = systems[s];
         const mgpu_grid &g = grids[s];
         const int b = bucket_for(c.n);
-        const int NT = kBucketNT[b];
-        const int npad = kT * NT;
+        const int npad = bucket_npad(b);
         const int nt = ntiles_of(b);
-        const int TT = kT * kT;
+        const size_t TT = tile_elems(b);
         p->sys_n.push_back(c.n);
         p->sys_bucket.push_back(b);
         p->sys_nstep.push_back(g.nstep);
         p->sys_nham.push_back(c.nham);
-        // VL / IV into the tile layout [term][element][tile]
+        // VL / IV into the bucket's tile layout
         const size_t tsz = (size_t)std::max(c.nham, 1) * TT * nt;
         std::vector<double> vlt(tsz, 0.0);
         std::vector<int> ivt(c.ivlfl > 0 ? tsz : 1, 0);
-        for (int t = 0; t < nt; ++t) {
-            int I = 0;
-            while ((I + 1) * (I + 2) / 2 <= t) ++I;
-            const int J = t - I * (I + 1) / 2;
-            for (int r = 0; r < kT; ++r)
-                for (int cc = 0; cc < kT; ++cc) {
-                    const int i = I * kT + r, j = J * kT + cc;
-                    if (i >= c.n || j >= c.n) continue;
-                    const int lo = std::min(i, j), hi = std::max(i, j);
-                    // pair (row lo, column hi) of the packed upper triangle (sumlam.f:33-36,74-86)
-                    const size_t pair = (size_t)hi * (hi + 1) / 2 + lo;
-                    for (int l = 0; l < c.nham; ++l) {
-                        const size_t src = pair * c.nvlblk + l;
-                        const size_t dst = ((size_t)l * TT + r * kT + cc) * nt + t;
-                        vlt[dst] = c.vl[src];
-                        if (c.ivlfl > 0) {
-                            int ix = c.iv[src] - 1;
-                            if (ix < 0 || ix >= c.nham) {
-                                delete p;
-                                return set_err(MGPU_ERR_ARG, "IV index outside 1..NHAM");
-                            }
-                            ivt[dst] = ix;
+        for (int t = 0; t < nt; ++t)
+            for (int ee = 0; ee < (int)TT; ++ee) {
+                int i = 0, j = 0;
+                tile_element(b, t, ee, &i, &j);
+                if (i >= c.n || j >= c.n) continue;
+                const int lo = std::min(i, j), hi = std::max(i, j);
+                // pair (row lo, column hi) of the packed upper triangle (sumlam.f:33-36,74-86)
+                const size_t pair = (size_t)hi * (hi + 1) / 2 + lo;
+                for (int l = 0; l < c.nham; ++l) {
+                    const size_t src = pair * c.nvlblk + l;
+                    const size_t dst = tile_offset(b, l, t, ee);
+                    vlt[dst] = c.vl[src];
+                    if (c.ivlfl > 0) {
+                        int ix = c.iv[src] - 1;
+                        if (ix < 0 || ix >= c.nham) {
+                            delete p;
+                            return set_err(MGPU_ERR_ARG, "IV index outside 1..NHAM");
                         }
+                        ivt[dst] = ix;
                     }
                 }
-        }
+            }
         std::vector<double> eint(npad, 0.0), cent(npad, 0.0);
         std::copy(c.eint, c.eint + c.n, eint.begin());
         std::copy(c.cent, c.cent + c.n, cent.begin());
@@ -873,6 +977,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         d.nrsq = c.nrsq;
         d.nstep = g.nstep;
         d.ntiles = nt;
+        d.kind = kBuckets[b].kind;
         d.conlen = c.conlen;
         d.dr = g.dr;
         const size_t nr = 2 * (size_t)g.nstep + 1;
@@ -966,14 +1071,10 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         p->sys_begin.push_back(sb);
         p->sys_count.push_back(sc);
         p->max_nstep.push_back(mx);
-        // shared memory: LDMD keeps two 2HQ(C) tile buffers; both kernels stage
-        // the VL tiles when they fit in the budget
-        const size_t tile_bytes = (size_t)kT * kT * ntiles_of(b) * sizeof(double);
-        const size_t base = iprop == MGPU_PROP_LDMD ? 2 * tile_bytes : 0;
-        const size_t vlb = (size_t)nhmax * tile_bytes;
-        const int use_vl = (base + vlb <= kSmemBudget) ? 1 : 0;
+        int use_vl = 0;
+        const size_t smem = prop_smem(iprop, b, nhmax, &use_vl);
         p->vl_smem.push_back(use_vl);
-        p->smem.push_back(base + (use_vl ? vlb : 0));
+        p->smem.push_back(smem);
     }
     if ((e = upload(p, &p->d_jobs, hj.data(), hj.size())) ||
         (e = upload(p, &p->d_syslists, syslist.data(), syslist.size()))) {
@@ -1005,8 +1106,8 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
         for (size_t b = 0; b < p->bucket_ids.size(); ++b) {
             if (p->sys_count[b] == 0) continue;
             for (int s0 = 0; s0 < p->sys_count[b]; s0 += 65535) {
-                dim3 grid(p->max_nstep[b], std::min(65535, p->sys_count[b] - s0));
-                if ((e = launch_prep(p->bucket_ids[b], grid, st, p->d_sys, p->d_syslists + p->sys_begin[b] + s0)))
+                if ((e = launch_prep(p->bucket_ids[b], p->max_nstep[b], std::min(65535, p->sys_count[b] - s0), st,
+                                     p->d_sys, p->d_syslists + p->sys_begin[b] + s0)))
                     return set_err(MGPU_ERR_CUDA, "launching ldmd_prep_kernel", e);
             }
         }
@@ -1118,9 +1219,9 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 __global__ void noalloc_setup_kernel(SysDev proto, SysDev *sys_out, JobDev *jobs, int njobs, const double *ered,
                                      int *syslist, const double *vl, const int *iv, int nvlblk, const double *eint,
                                      const double *cent, double *eint_p, double *cent_p, double *vlt, int *ivt,
-                                     int npad, int T)
+                                     int npad, int edge)
 {
-    const int TT = T * T;
+    const int TT = edge * edge;
     const int nt = proto.ntiles;
     const size_t nvlt = (size_t)proto.nham * TT * nt;
     const size_t total = nvlt > (size_t)njobs ? nvlt : (size_t)njobs;
@@ -1146,13 +1247,29 @@ __global__ void noalloc_setup_kernel(SysDev proto, SysDev *sys_out, JobDev *jobs
             cent_p[x] = x < (size_t)proto.n ? cent[x] : 0.0;
         }
         if (x < nvlt) {
-            const int t = (int)(x % nt);
-            const int e = (int)((x / nt) % TT);
-            const int l = (int)(x / ((size_t)nt * TT));
+            // x enumerates the destination array in its own layout
+            int l, t, e;
+            if (proto.kind == 1) {  // [term][tile][lane][s]
+                e = (int)(x % TT);
+                t = (int)((x / TT) % nt);
+                l = (int)(x / ((size_t)TT * nt));
+            } else {  // [term][element][tile]
+                t = (int)(x % nt);
+                e = (int)((x / nt) % TT);
+                l = (int)(x / ((size_t)nt * TT));
+            }
             int I = 0;
             while ((I + 1) * (I + 2) / 2 <= t) ++I;
             const int J = t - I * (I + 1) / 2;
-            const int i = I * T + e / T, j = J * T + e % T;
+            int i, j;
+            if (proto.kind == 1) {
+                const int lane = e >> 1, s2 = e & 1;
+                i = 8 * I + (lane >> 2);
+                j = 8 * J + 2 * (lane & 3) + s2;
+            } else {
+                i = I * edge + e / edge;
+                j = J * edge + e % edge;
+            }
             double v = 0.0;
             int ix = 0;
             if (i < proto.n && j < proto.n) {
@@ -1189,8 +1306,8 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
     const int b = bucket_for(c->n);
     if (b < 0) return set_err(MGPU_ERR_UNSUPPORTED, "N above the largest compiled bucket");
     const int nt = ntiles_of(b);
-    const int npad = kT * kBucketNT[b];
-    const size_t tile = (size_t)kT * kT * nt;  // doubles per tiled matrix
+    const int npad = bucket_npad(b);
+    const size_t tile = matrix_elems(b);  // doubles per tiled matrix
 
     // scratch layout
     size_t off = 0;
@@ -1243,6 +1360,7 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
     proto.nrsq = c->nrsq;
     proto.nstep = g->nstep;
     proto.ntiles = nt;
+    proto.kind = kBuckets[b].kind;
     proto.conlen = c->conlen;
     proto.dr = g->dr;
     proto.vlt = reinterpret_cast<double *>(base + o_vlt);
@@ -1263,14 +1381,12 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
     noalloc_setup_kernel<<<blocks, 256, 0, st>>>(proto, d_sys, d_jobs, njobs, ered_dev, d_list, c->vl, c->iv,
                                                  c->nvlblk, c->eint, c->cent, const_cast<double *>(proto.eint),
                                                  const_cast<double *>(proto.cent), const_cast<double *>(proto.vlt),
-                                                 const_cast<int *>(proto.ivt), npad, kT);
+                                                 const_cast<int *>(proto.ivt), npad, bucket_edge(b));
     if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching noalloc_setup_kernel", e);
-    if ((e = launch_prep(b, dim3(g->nstep, 1), st, d_sys, d_list)))
+    if ((e = launch_prep(b, g->nstep, 1, st, d_sys, d_list)))
         return set_err(MGPU_ERR_CUDA, "launching ldmd_prep_kernel", e);
-    const size_t tile_bytes = tile * sizeof(double);
-    const size_t vlb = (size_t)c->nham * tile_bytes;
-    const int use_vl = (2 * tile_bytes + vlb <= kSmemBudget) ? 1 : 0;
-    const size_t smem = 2 * tile_bytes + (use_vl ? vlb : 0);
+    int use_vl = 0;
+    const size_t smem = prop_smem(MGPU_PROP_LDMD, b, c->nham, &use_vl);
     if ((e = launch_prop(MGPU_PROP_LDMD, b, njobs, smem, use_vl, st, d_sys, d_jobs, y_dev, nodes_dev, status_dev,
                          kfail_dev)))
         return set_err(MGPU_ERR_CUDA, "launching ldmd_prop_kernel", e);
