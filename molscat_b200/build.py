@@ -7,6 +7,7 @@ object (include/molscat_gpu.h); Python reaches it through ctypes.
 """
 from __future__ import annotations
 
+import glob
 import os
 import subprocess
 import sys
@@ -15,7 +16,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libmolscat_gpu.so")
 SOURCES = [os.path.join(PKG, "csrc", "propagator.cu")]
-DEPS = SOURCES + [os.path.join(PKG, "csrc", "tiles.cuh"), os.path.join(ROOT, "include", "molscat_gpu.h")]
+DEPS = SOURCES + sorted(glob.glob(os.path.join(PKG, "csrc", "*.cuh"))) + [os.path.join(ROOT, "include", "molscat_gpu.h")]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",

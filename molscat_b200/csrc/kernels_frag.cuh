@@ -13,13 +13,13 @@ namespace wf {
 
 constexpr int kWPB = 4;  // warps (matrices) per CTA
 
-// per-warp shared memory (doubles): panel, y14, y14', y23, two 2HQ(C) buffers
+// per-warp shared memory (doubles): panel, y14, y14', y23, the 2HQ(C) tile
 template <int NT>
 struct WarpSmem {
     static constexpr int PAN = G<NT>::WSM;
     static constexpr int VEC = G<NT>::NPAD;
     static constexpr int QD = G<NT>::NTL * 64;
-    static constexpr int DOUBLES = PAN + 3 * VEC + 2 * QD;
+    static constexpr int DOUBLES = PAN + 3 * VEC + QD;
     static constexpr size_t BYTES = (size_t)DOUBLES * 8;
 };
 
@@ -76,68 +76,6 @@ __device__ __forceinline__ void w_frag(const SysDev &S, int lane, int ir, double
                 }
             }
     }
-}
-
-// a <- dd * W(R) + yr_I a yc_J (+ y14' on the diagonal), one tile at a time
-// so W never lives in registers as a whole (mdprop.f:196-230).
-template <int NT>
-__device__ __forceinline__ void apply_wb_frag(const SysDev &S, int lane, int ir, double ered, double dd,
-                                              const double (&yr)[NT], const double (&yc)[NT][2],
-                                              const double *__restrict__ s_y14b, double (&a)[G<NT>::NTL][2])
-{
-    constexpr int NTL = G<NT>::NTL;
-    const double *P = S.ptab + (size_t)ir * S.nham;
-    const double R = __ldg(S.rtab + ir);
-    const double rsq = fmin(1.0 / (R * R), 1.0e16);
-    double conf = 0.0;
-    if (S.conlen > 0.0) {
-        const double c2 = S.conlen * S.conlen;
-        conf = R * R / (c2 * c2);
-    }
-    const int r = lane >> 2, q = lane & 3;
-#pragma unroll
-    for (int I = 0; I < NT; ++I)
-#pragma unroll
-        for (int J = 0; J <= I; ++J) {
-            const int t = tix(I, J);
-            double w0 = 0.0, w1 = 0.0;
-            const double *v = S.vlt + (size_t)t * 64 + lane * 2;
-            if (S.ivlfl <= 0) {
-                for (int l = 0; l < S.nham; ++l) {
-                    const double2 x = __ldg(reinterpret_cast<const double2 *>(v + (size_t)l * NTL * 64));
-                    const double pl = __ldg(P + l);
-                    w0 = fma(x.x, pl, w0);
-                    w1 = fma(x.y, pl, w1);
-                }
-            } else {
-                const int *iv = S.ivt + (size_t)t * 64 + lane * 2;
-                for (int l = 0; l < S.nham; ++l) {
-                    const double x0 = __ldg(v + (size_t)l * NTL * 64), x1 = __ldg(v + (size_t)l * NTL * 64 + 1);
-                    if (x0 != 0.0) w0 = fma(x0, __ldg(P + __ldg(iv + (size_t)l * NTL * 64)), w0);
-                    if (x1 != 0.0) w1 = fma(x1, __ldg(P + __ldg(iv + (size_t)l * NTL * 64 + 1)), w1);
-                }
-            }
-            if (I == J) {
-#pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    const int i = 8 * I + r;
-                    if (r == 2 * q + s && i < S.n) {
-                        double x = s ? w1 : w0;
-                        if (S.nrsq == 0) x += rsq * S.cent[i];
-                        if (S.nconst == 0) x += S.eint[i];
-                        if (S.conlen > 0.0) x += conf;
-                        x -= ered;
-                        if (s) w1 = x; else w0 = x;
-                    }
-                }
-            }
-            a[t][0] = dd * w0 + yr[I] * a[t][0] * yc[J][0];
-            a[t][1] = dd * w1 + yr[I] * a[t][1] * yc[J][1];
-            if (I == J) {
-                if (r == 2 * q) a[t][0] += s_y14b[8 * I + r];
-                if (r == 2 * q + 1) a[t][1] += s_y14b[8 * I + r];
-            }
-        }
 }
 
 // W(R)_ii (the DIAG array of HAMMAT) for channel i.
@@ -260,7 +198,7 @@ ldmd_prep_frag_kernel(const SysDev *__restrict__ systems, const int *__restrict_
 // MDPROP step loop, one warp per job.
 // ---------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(32 * kWPB, 3)
+__global__ void __launch_bounds__(32 * kWPB)
 ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs,
                       double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
                       int *__restrict__ kfail_out)
@@ -269,7 +207,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     constexpr int NPAD = G<NT>::NPAD;
     using W = WarpSmem<NT>;
     extern __shared__ __align__(16) double dsm[];
-    __shared__ __align__(8) uint64_t qbar[kWPB][2];
+    __shared__ __align__(8) uint64_t qbar[kWPB];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int jix = blockIdx.x * kWPB + warp;
     if (jix >= njobs) return;  // whole warp; the kernel has no CTA-wide barrier
@@ -284,7 +222,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     const int nstep = S.nstep;
     const double ered = job.ered;
     const uint32_t qbytes = (uint32_t)(NTL * 64 * sizeof(double));
-    uint64_t *bar = qbar[warp];
+    uint64_t *bar = &qbar[warp];
 
     if (S.prep[1] != 0) {
         if (lane == 0) {
@@ -296,12 +234,11 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     }
     for (int i = lane; i < NPAD; i += 32) s_y14[i] = s_y14b[i] = s_y23[i] = 0.0;
     if (lane == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        mbar_init(bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    if (lane == 0) bulk_load(qbuf + NTL * 64, S.q, qbytes, &bar[1]);  // 2HQ(C_1) -> buffer 1
+    if (lane == 0) bulk_load(qbuf, S.q, qbytes, bar);  // 2HQ(C_1); copy m completes phase m&1
 
     const double h = S.dr / 2.0;
     const double d1 = h * h / 3.0;
@@ -323,12 +260,6 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     int nodes = 0, status = MGPU_OK, kfail = 0;
     int issued = 1, consumed = 0;
     for (int k = 1; k <= nstep; ++k) {
-        const int sb = k & 1;
-        if (lane == 0 && k + 1 <= nstep) {
-            fence_async_shared();
-            bulk_load(qbuf + ((k + 1) & 1) * NTL * 64, S.q + (size_t)k * NTL * 64, qbytes, &bar[(k + 1) & 1]);
-            issued = k + 1;
-        }
         // reference-potential solutions in the sector (mdprop.f:143-164)
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
@@ -352,7 +283,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
             kfail = k;
             break;
         }
-        const bool landed = mbar_wait_bounded(&bar[sb], ((k - 1) >> 1) & 1);
+        const bool landed = mbar_wait_bounded(bar, (k - 1) & 1);
         if (__any_sync(0xffffffffu, !landed)) {
             status = MGPU_ERR_TIMEOUT;
             kfail = k;
@@ -367,7 +298,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
             yc[I][1] = s_y23[8 * I + 2 * q + 1];
         }
         {
-            const double *qs = qbuf + sb * NTL * 64 + lane * 2;
+            const double *qs = qbuf + lane * 2;
             // Y = 2HQ(C) + 2 Y14 - Y23 Y^-1 Y23   (a holds -Y^-1), mdprop.f:156,181-185
 #pragma unroll
             for (int I = 0; I < NT; ++I)
@@ -383,17 +314,41 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
                 for (int s = 0; s < 2; ++s)
                     if (r == 2 * q + s) a[tix(I, I)][s] += 2.0 * s_y14[8 * I + r];
         }
+        // every lane has read 2HQ(C_k): the async proxy may refill the buffer
+        __syncwarp();
+        if (lane == 0 && k + 1 <= nstep) {
+            fence_async_shared();
+            bulk_load(qbuf, S.q + (size_t)k * NTL * 64, qbytes, bar);
+            issued = k + 1;
+        }
         nodes += warp_sweep_invert<NT>(a, pan, n, lane, bad);
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
             break;
         }
-        // Y = D2 W(B) - Y23 Y^-1 Y23 + Y14'   (mdprop.f:196-230)
-        apply_wb_frag<NT>(S, lane, 2 * k, ered, (k == nstep) ? d1 : d2, yr, yc, s_y14b, a);
+        {
+            const double dd = (k == nstep) ? d1 : d2;
+            double w[NTL][2];
+            w_frag<NT>(S, lane, 2 * k, ered, true, w);
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int J = 0; J <= I; ++J)
+#pragma unroll
+                    for (int s = 0; s < 2; ++s)
+                        a[tix(I, J)][s] = dd * w[tix(I, J)][s] + yr[I] * a[tix(I, J)][s] * yc[J][s];
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+                    if (r == 2 * q + s) a[tix(I, I)][s] += s_y14b[8 * I + r];
+        }
     }
-    if (status != MGPU_OK && lane == 0) {
-        for (int s2 = consumed + 1; s2 <= issued; ++s2) mbar_wait_bounded(&bar[s2 & 1], ((s2 - 1) >> 1) & 1);
+    if (status != MGPU_OK && lane == 0 && issued > consumed) {
+        // an early exit can leave one copy in flight: let it land (bounded)
+        // before this warp's shared memory can be reused
+        mbar_wait_bounded(bar, (issued - 1) & 1);
     }
     __syncwarp();
     if (status == MGPU_OK) store_full_frag<NT>(yj, n, lane, 1.0 / h, a);
