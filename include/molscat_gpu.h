@@ -168,10 +168,16 @@ int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, int njobs,
                         const double *ered_dev, double *y_dev, int *nodes_dev,
                         int *status_dev, int *kfail_dev, void *stream);
 
+/* Kernel family for the sizes two families cover (N <= 64): 0 = FP64
+ * tensor-core (DMMA) 8x8 fragments, one warp (N <= 40) or one CTA per
+ * matrix (the default); 1 = 4x4 register tiles with the scalar sweep.
+ * Affects plans created afterwards; returns the previous setting. */
+int mgpu_set_kernel_family(int family);
+
 /* ---- diagnostics --------------------------------------------------------- */
 const char *mgpu_status_string(int status);
 const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */
-int mgpu_max_n(void);                /* largest N the compiled buckets accept */
+int mgpu_max_n(void);                /* largest N MDPROP accepts (LDPROP: 128) */
 
 #ifdef __cplusplus
 }

@@ -44,7 +44,7 @@ EXPORTS = (
     "mgpu_plan_create", "mgpu_plan_destroy", "mgpu_plan_y_elems", "mgpu_plan_y_offset",
     "mgpu_plan_flops", "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
     "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
-    "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc",
+    "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc", "mgpu_set_kernel_family",
 )
 
 _lib = None
@@ -87,9 +87,19 @@ def load(path: str | None = None):
     L.mgpu_last_error.argtypes = []
     L.mgpu_last_error.restype = ctypes.c_char_p
     L.mgpu_max_n.argtypes = []
+    L.mgpu_set_kernel_family.argtypes = [ctypes.c_int]
     if path is None:
         _lib = L
     return L
+
+
+FAMILY_DMMA = 0
+FAMILY_TILE4 = 1
+
+
+def set_kernel_family(family: int) -> int:
+    """Kernel family for N <= 64 (FAMILY_DMMA default, FAMILY_TILE4); returns the old one."""
+    return int(load().mgpu_set_kernel_family(int(family)))
 
 
 def last_error() -> str:

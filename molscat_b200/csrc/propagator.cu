@@ -547,6 +547,7 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
 
 }  // namespace mgpu
 #include "kernels_frag.cuh"
+#include "kernels_cta.cuh"
 namespace mgpu {
 
 __global__ void prep_reset_kernel(int *prep, int nsys)
@@ -583,39 +584,57 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int it
 // ---------------------------------------------------------------------------
 #define MGPU_BUCKETS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(12) X(14) X(16)
 #define MGPU_FRAG_BUCKETS(X) X(1) X(2) X(3) X(4) X(5)
+// (NT, warps) of the one-CTA-per-matrix buckets, N = 8*NT up to 200
+#define MGPU_CTA_BUCKETS(X) X(6, 4) X(7, 4) X(8, 4) X(10, 8) X(12, 8) X(14, 8) X(16, 8) X(20, 16) X(25, 16)
 
-enum { KIND_TILE4 = 0, KIND_FRAG8 = 1 };
+// KIND_FRAG8: one warp per matrix; KIND_CTA8: one CTA per matrix (same 8x8
+// fragment data layout); KIND_TILE4: 4x4 register tiles.
+enum { KIND_TILE4 = 0, KIND_FRAG8 = 1, KIND_CTA8 = 2 };
 
 struct Bucket {
     int kind;
     int nt;
+    int warps;  // KIND_CTA8
 };
 
-// 8x8-fragment buckets first (preferred for N <= 40), then 4x4 register tiles.
+// 8x8-fragment buckets first (one warp for N <= 40, one CTA up to 200), then
+// the 4x4 register tiles (N <= 64).
 static const Bucket kBuckets[] = {
-#define X(nt) {KIND_FRAG8, nt},
+#define X(nt) {KIND_FRAG8, nt, 1},
     MGPU_FRAG_BUCKETS(X)
 #undef X
-#define X(nt) {KIND_TILE4, nt},
+#define X(nt, w) {KIND_CTA8, nt, w},
+    MGPU_CTA_BUCKETS(X)
+#undef X
+#define X(nt) {KIND_TILE4, nt, 0},
     MGPU_BUCKETS(X)
 #undef X
 };
 static const int kNumBuckets = sizeof(kBuckets) / sizeof(kBuckets[0]);
 
-static int bucket_edge(int b) { return kBuckets[b].kind == KIND_FRAG8 ? 8 : kT; }
+static bool frag_layout(int b) { return kBuckets[b].kind != KIND_TILE4; }
+static int bucket_edge(int b) { return frag_layout(b) ? 8 : kT; }
 static int bucket_npad(int b) { return bucket_edge(b) * kBuckets[b].nt; }
 static int ntiles_of(int b) { return kBuckets[b].nt * (kBuckets[b].nt + 1) / 2; }
 static size_t tile_elems(int b) { return (size_t)bucket_edge(b) * bucket_edge(b); }  // doubles per tile
 static size_t matrix_elems(int b) { return tile_elems(b) * ntiles_of(b); }         // doubles per tiled matrix
 
-// Smallest bucket of the preferred kind that holds N (falls back to the other kind).
-static int g_prefer_kind = KIND_FRAG8;
-static int bucket_for(int n)
+// LDJ keeps two tiled matrices in shared memory: CTA buckets up to N = 128.
+static bool bucket_allows(int b, int iprop)
+{
+    return !(iprop == MGPU_PROP_LDJ && kBuckets[b].kind == KIND_CTA8 && kBuckets[b].nt > 16);
+}
+
+// Smallest bucket that holds N: the fragment kernels first, then the 4x4
+// register tiles; g_prefer_tile4 puts the 4x4 tiles first where they fit.
+static int g_prefer_tile4 = 0;
+static int bucket_for(int n, int iprop = MGPU_PROP_LDMD)
 {
     for (int pass = 0; pass < 2; ++pass) {
-        const int kind = pass == 0 ? g_prefer_kind : 1 - g_prefer_kind;
+        const bool tile4 = (pass == 0) == (g_prefer_tile4 != 0);
         for (int b = 0; b < kNumBuckets; ++b)
-            if (kBuckets[b].kind == kind && bucket_npad(b) >= n) return b;
+            if ((kBuckets[b].kind == KIND_TILE4) == tile4 && bucket_npad(b) >= n && bucket_allows(b, iprop))
+                return b;
     }
     return -1;
 }
@@ -634,6 +653,23 @@ static cudaError_t set_smem(K kernel, size_t bytes)
 static cudaError_t launch_prep(int b, int max_nstep, int nsys, cudaStream_t st, const SysDev *sys, const int *list)
 {
     const int nt = kBuckets[b].nt;
+    if (kBuckets[b].kind == KIND_CTA8) {
+        dim3 grid(max_nstep, nsys);
+        cudaError_t e = cudaSuccess;
+        switch (nt) {
+#define X(t, w)                                                                                   \
+    case t: {                                                                                     \
+        const size_t sm = cta::CSmem<t, w>::bytes(1);                                             \
+        if ((e = set_smem(cta::ldmd_prep_cta_kernel<t, w>, sm))) return e;                        \
+        cta::ldmd_prep_cta_kernel<t, w><<<grid, 32 * w, sm, st>>>(sys, list);                    \
+        break;                                                                                    \
+    }
+            MGPU_CTA_BUCKETS(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     if (kBuckets[b].kind == KIND_FRAG8) {
         dim3 grid((max_nstep + wf::kWPB - 1) / wf::kWPB, nsys);
         switch (nt) {
@@ -662,6 +698,15 @@ static cudaError_t launch_prep(int b, int max_nstep, int nsys, cudaStream_t st, 
 // 4x4-tile kernels stage VL when it fits).
 static size_t prop_smem(int iprop, int b, int nham, int *vl_smem)
 {
+    if (kBuckets[b].kind == KIND_CTA8) {
+        *vl_smem = 0;
+        switch (kBuckets[b].nt) {
+#define X(t, w) case t: return cta::CSmem<t, w>::bytes(iprop == MGPU_PROP_LDJ ? 2 : 1);
+            MGPU_CTA_BUCKETS(X)
+#undef X
+        }
+        return 0;
+    }
     if (kBuckets[b].kind == KIND_FRAG8) {
         *vl_smem = 0;
         size_t per = 0;
@@ -684,6 +729,24 @@ static cudaError_t launch_prop(int iprop, int b, int njobs, size_t smem, int vl_
 {
     cudaError_t e = cudaSuccess;
     const int nt = kBuckets[b].nt;
+    if (kBuckets[b].kind == KIND_CTA8) {
+        switch (nt) {
+#define X(t, w)                                                                                              \
+    case t:                                                                                                  \
+        if (iprop == MGPU_PROP_LDMD) {                                                                       \
+            if ((e = set_smem(cta::ldmd_prop_cta_kernel<t, w>, smem))) return e;                             \
+            cta::ldmd_prop_cta_kernel<t, w><<<njobs, 32 * w, smem, st>>>(sys, jobs, y, nodes, status, kfail); \
+        } else {                                                                                             \
+            if ((e = set_smem(cta::ldj_prop_cta_kernel<t, w>, smem))) return e;                              \
+            cta::ldj_prop_cta_kernel<t, w><<<njobs, 32 * w, smem, st>>>(sys, jobs, y, nodes, status, kfail);  \
+        }                                                                                                    \
+        break;
+            MGPU_CTA_BUCKETS(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+        }
+        return cudaGetLastError();
+    }
     if (kBuckets[b].kind == KIND_FRAG8) {
         const int blocks = (njobs + wf::kWPB - 1) / wf::kWPB;
         switch (nt) {
@@ -730,7 +793,7 @@ static void tile_element(int b, int t, int e, int *i, int *j)
     int I = 0;
     while ((I + 1) * (I + 2) / 2 <= t) ++I;
     const int J = t - I * (I + 1) / 2;
-    if (kBuckets[b].kind == KIND_FRAG8) {
+    if (frag_layout(b)) {
         const int lane = e >> 1, s = e & 1;
         *i = 8 * I + (lane >> 2);
         *j = 8 * J + 2 * (lane & 3) + s;
@@ -744,7 +807,7 @@ static void tile_element(int b, int t, int e, int *i, int *j)
 static size_t tile_offset(int b, int l, int t, int e)
 {
     const int nt = ntiles_of(b);
-    if (kBuckets[b].kind == KIND_FRAG8) return ((size_t)l * nt + t) * 64 + e;
+    if (frag_layout(b)) return ((size_t)l * nt + t) * 64 + e;
     return ((size_t)l * tile_elems(b) + e) * nt + t;
 }
 
@@ -820,7 +883,7 @@ static cudaError_t upload(mgpu_plan *p, X **dst, const X *src, size_t count)
     return e;
 }
 
-static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g)
+static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g, int iprop)
 {
     if (!c || !g) return set_err(MGPU_ERR_ARG, "null system or grid");
     if (c->n < 1) return set_err(MGPU_ERR_ARG, "N must be >= 1");
@@ -831,7 +894,9 @@ static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g)
     if (g->nstep < 1) return set_err(MGPU_ERR_ARG, "NSTEP must be >= 1");
     if (!g->rtab || (c->nham > 0 && !g->ptab)) return set_err(MGPU_ERR_ARG, "radial tables null");
     if (!(g->dr != 0.0) || !std::isfinite(g->dr)) return set_err(MGPU_ERR_ARG, "DR must be finite and non-zero");
-    if (bucket_for(c->n) < 0) return set_err(MGPU_ERR_UNSUPPORTED, "N above the largest compiled bucket");
+    if (bucket_for(c->n, iprop) < 0)
+        return set_err(MGPU_ERR_UNSUPPORTED, iprop == MGPU_PROP_LDJ ? "N above 128 (largest LDPROP bucket)"
+                                                                     : "N above 200 (largest MDPROP bucket)");
     return MGPU_OK;
 }
 
@@ -842,6 +907,13 @@ int mgpu_max_n(void)
     int m = 0;
     for (int b = 0; b < kNumBuckets; ++b) m = std::max(m, bucket_npad(b));
     return m;
+}
+
+int mgpu_set_kernel_family(int family)
+{
+    const int old = g_prefer_tile4;
+    g_prefer_tile4 = family == 1 ? 1 : 0;
+    return old;
 }
 
 int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out)
@@ -914,7 +986,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     if (nsys < 1 || njobs < 0 || !systems || !grids || (njobs > 0 && (!job_sys || !job_ered)))
         return set_err(MGPU_ERR_ARG, "bad system/job arrays");
     for (int s = 0; s < nsys; ++s) {
-        int rc = check_coupling(&systems[s], &grids[s]);
+        int rc = check_coupling(&systems[s], &grids[s], iprop);
         if (rc) return rc;
     }
     for (int j = 0; j < njobs; ++j)
@@ -934,7 +1006,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     for (int s = 0; s < nsys; ++s) {
         const mgpu_coupling &c = systems[s];
         const mgpu_grid &g = grids[s];
-        const int b = bucket_for(c.n);
+        const int b = bucket_for(c.n, iprop);
         const int npad = bucket_npad(b);
         const int nt = ntiles_of(b);
         const size_t TT = tile_elems(b);
@@ -980,7 +1052,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         d.nrsq = c.nrsq;
         d.nstep = g.nstep;
         d.ntiles = nt;
-        d.kind = kBuckets[b].kind;
+        d.kind = frag_layout(b) ? 1 : 0;
         d.conlen = c.conlen;
         d.dr = g.dr;
         const size_t nr = 2 * (size_t)g.nstep + 1;
@@ -1363,7 +1435,7 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
     proto.nrsq = c->nrsq;
     proto.nstep = g->nstep;
     proto.ntiles = nt;
-    proto.kind = kBuckets[b].kind;
+    proto.kind = frag_layout(b) ? 1 : 0;
     proto.conlen = c->conlen;
     proto.dr = g->dr;
     proto.vlt = reinterpret_cast<double *>(base + o_vlt);

@@ -74,7 +74,7 @@ __device__ __forceinline__ double pivot_reciprocal(double d)
 // part (equal by symmetry) in tile row K.  Branch-free: predicated stores and
 // selects, so threads that own nothing of row/column k run the same code.
 template <int T, int NPAD, int KK>
-__device__ __forceinline__ void publish_clear_kk(double (&a)[T][T], double *__restrict__ dst, int K, int I, int J,
+__device__ __forceinline__ void publish_clear_kk(double (&a)[T][T], double *dst, int K, int I, int J,
                                                  bool act = true)
 {
     const bool colown = act && (J == K);            // publishes a[.][KK]: column k, rows of tile row I
@@ -96,7 +96,7 @@ __device__ __forceinline__ void publish_clear_kk(double (&a)[T][T], double *__re
 }
 
 template <int T, int NPAD>
-__device__ __forceinline__ void publish_clear(double (&a)[T][T], double *__restrict__ dst, int k, int I, int J)
+__device__ __forceinline__ void publish_clear(double (&a)[T][T], double *dst, int k, int I, int J)
 {
     const int K = k / T;
     switch (k - K * T) {
@@ -125,7 +125,7 @@ __device__ __forceinline__ int flags_to_status(int f)
 // One pivot of the sweep, pivot k = K*T + KK with KK a compile-time constant
 // (register indices are static; no switch, no branch on data).
 template <int T, int NT, int KK>
-__device__ __forceinline__ void sweep_pivot(double (&a)[T][T], double *__restrict__ vb, int k, int K, int n, int I,
+__device__ __forceinline__ void sweep_pivot(double (&a)[T][T], double *vb, int k, int K, int n, int I,
                                             int J, bool act, int &cnt, int &flags)
 {
     constexpr int NPAD = Geom<T, NT>::NPAD;
@@ -164,7 +164,7 @@ __device__ __forceinline__ void sweep_pivot(double (&a)[T][T], double *__restric
 // SWEEP_NONFINITE if a pivot failed (identical in every thread).  After a
 // failed pivot the remaining arithmetic runs on inf/NaN and is discarded.
 template <int T, int NT>
-__device__ __forceinline__ int sweep_invert(double (&a)[T][T], double *__restrict__ vb, int n, int I, int J,
+__device__ __forceinline__ int sweep_invert(double (&a)[T][T], double *vb, int n, int I, int J,
                                             bool act, int &bad)
 {
     static_assert(T >= 1 && T <= 4, "tile edge 1..4");
@@ -186,8 +186,8 @@ __device__ __forceinline__ int sweep_invert(double (&a)[T][T], double *__restric
 // Two independent matrices inverted together (one barrier per pivot serves
 // both).  Returns a's negative pivots; b's go to cnt_b.
 template <int T, int NT, int KK>
-__device__ __forceinline__ void sweep_pivot2(double (&a)[T][T], double (&b)[T][T], double *__restrict__ va,
-                                             double *__restrict__ vbb, int k, int K, int n, int I, int J, bool act,
+__device__ __forceinline__ void sweep_pivot2(double (&a)[T][T], double (&b)[T][T], double *va,
+                                             double *vbb, int k, int K, int n, int I, int J, bool act,
                                              int &ca, int &cb, int &flags)
 {
     constexpr int NPAD = Geom<T, NT>::NPAD;
@@ -224,8 +224,8 @@ __device__ __forceinline__ void sweep_pivot2(double (&a)[T][T], double (&b)[T][T
 }
 
 template <int T, int NT>
-__device__ __forceinline__ int sweep_invert2(double (&a)[T][T], double (&b)[T][T], double *__restrict__ va,
-                                             double *__restrict__ vbb, int n, int I, int J, bool act, int &cnt_b,
+__device__ __forceinline__ int sweep_invert2(double (&a)[T][T], double (&b)[T][T], double *va,
+                                             double *vbb, int n, int I, int J, bool act, int &cnt_b,
                                              int &bad)
 {
     constexpr int NPAD = Geom<T, NT>::NPAD;

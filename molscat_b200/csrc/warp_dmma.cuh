@@ -7,24 +7,28 @@
 // triangles.  Padding rows/columns are zero.
 //
 // Inversion is the symmetric Gauss-Jordan sweep done four pivots at a time
-// (block sweep).  For the pivot block P = {p0..p0+3} with D = A_PP and
-// F = -D^{-1}:
-//     A_ij += (A_iP F) A_Pj          i,j not in P
-//     A_iP  = -(A_iP F) ,  A_Pj = -(F A_Pj) ,  A_PP = F
-// which after all blocks leaves -A^{-1} (the same result as the scalar sweep
-// in tiles.cuh).  As there, the owners zero row/column block P and the
-// operands carry the pivot block, so every tile gets the same update
+// (block sweep).  For the pivot block P = {p0..p0+3} with D = A_PP = L Delta L^T
+// (unpivoted, the scalar sweep's own pivots delta_k) and Lam = L^{-1}:
+//     c_k(i) = sum_m Lam[k][m] A_{i,p0+m}          (i not in P)
+//     A_ij  -= sum_k c_k(i) c_k(j) / delta_k        (i, j not in P)
+//     A_iP   = A_iP D^{-1} ,  A_PP = -D^{-1}
+// which after all blocks leaves -A^{-1}.  The trailing update is the scalar
+// sweep's own sum of rank-one terms, so the block sweep keeps its rounding
+// behaviour; forming D^{-1} first and updating with A_iP D^{-1} A_Pj instead
+// loses accuracy when a pivot is small next to its neighbours.  As in
+// tiles.cuh the owners zero row/column block P and the operands carry the
+// pivot block, so every lower tile gets the same update
 //     A_IJ += X_I B_J          (one m8n8k4 DMMA per lower tile)
-// with X_I = A_{I,P} F (rows of P replaced by -F) and B_J = A_{P,J}
-// (columns of P replaced by -I).  The panel A_{:,P} goes through a small
-// per-warp shared-memory buffer.
+// with X(i,k) = -c_k(i)/delta_k, B(j,k) = c_k(j) for rows outside P and
+// X(p0+a,k) = Lam[k][a]/delta_k, B(p0+b,k) = -Lam[k][b] for rows of P, which
+// writes A_iP D^{-1} into the columns of P and -D^{-1} into A_PP.  The panel
+// A_{:,P} goes through a small per-warp shared-memory buffer.  Every read of
+// a diagonal tile takes the lower triangle, so the stored matrix is symmetric
+// for the algorithm whatever rounding left in the upper triangle.
 //
-// F comes from D by 2x2 blocks (two reciprocals per block of four pivots).
-// The pivots of that block LDL^T are those of the unpivoted LDL^T SYMINV
-// forms (syminv.f:27-49): d1 = a00, d2 = det(A)/a00 for the leading 2x2 A,
-// d3, d4 likewise for the Schur complement S = C - B A^{-1} B^T.  Their
-// negative count is SYMINV's KOUNT (and DSYNEG's inertia by Sylvester's
-// law); a zero a00 or det is the reference's IFAIL = N+1.
+// The pivots delta_k are those of the unpivoted LDL^T SYMINV forms
+// (syminv.f:27-49); their negative count is SYMINV's KOUNT (and DSYNEG's
+// inertia by Sylvester's law); a zero pivot is the reference's IFAIL = N+1.
 #pragma once
 #include <cuda_runtime.h>
 #include <float.h>
@@ -53,59 +57,52 @@ __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-// -D^{-1} of a symmetric 4x4 block by 2x2 blocks, counting negative pivots
-// of the first `nreal` rows (the rest are padding and are treated as 1).
-__device__ __forceinline__ void neg_inverse4(double d[4][4], int nreal, int &cnt, int &flags)
+// Unpivoted LDL^T of the symmetric 4x4 pivot block D, read from the lower
+// triangle of d (the upper triangle is ignored), pivot by pivot as the scalar
+// sweep meets them.  On return d holds the block's operands:
+//     d[k][k] = 1/delta_k ,  d[i][k] = Lam[i][k] (i > k) ,  d[k][i] = 0
+// with Lam = L^{-1} (unit lower).  Negative pivots of the first `nreal` rows
+// are added to cnt; the rest are padding, zero off the diagonal, and taken as
+// exact unit pivots (not counted, never singular).
+__device__ __forceinline__ void ldl_block4(double d[4][4], int nreal, int &cnt, int &flags)
 {
-    // padding rows/columns of the matrix are zero off the diagonal; a padding
-    // pivot is taken as exactly 1 (not counted, never singular)
 #pragma unroll
     for (int i = 0; i < 4; ++i) d[i][i] = (i >= nreal) ? 1.0 : d[i][i];
-    // leading 2x2 block A
-    const double a00 = d[0][0], a01 = d[1][0], a11 = d[1][1];
-    const double detA = fma(a00, a11, -a01 * a01);
-    const double rA = pivot_reciprocal(detA);
-    const double i00 = a11 * rA, i01 = -a01 * rA, i11 = a00 * rA;  // A^{-1}
-    // W = B A^{-1}, B = rows 2,3 x cols 0,1
-    const double b00 = d[2][0], b01 = d[2][1], b10 = d[3][0], b11 = d[3][1];
-    const double w00 = fma(b00, i00, b01 * i01), w01 = fma(b00, i01, b01 * i11);
-    const double w10 = fma(b10, i00, b11 * i01), w11 = fma(b10, i01, b11 * i11);
-    // Schur complement S = C - W B^T
-    const double s00 = d[2][2] - fma(w00, b00, w01 * b01);
-    const double s01 = d[3][2] - fma(w10, b00, w11 * b01);
-    const double s11 = d[3][3] - fma(w10, b10, w11 * b11);
-    const double detS = fma(s00, s11, -s01 * s01);
-    const double rS = pivot_reciprocal(detS);
-    const double j00 = s11 * rS, j01 = -s01 * rS, j11 = s00 * rS;  // S^{-1}
-    // pivots d1 = a00, d2 = detA/a00, d3 = s00, d4 = detS/s00 (padding rows are
-    // exact unit pivots: positive, finite, so counting all four is exact)
-    flags |= pivot_flags(a00) | pivot_flags(detA) | pivot_flags(s00) | pivot_flags(detS);
-    cnt += (a00 < 0.0) + ((detA < 0.0) != (a00 < 0.0)) + (s00 < 0.0) + ((detS < 0.0) != (s00 < 0.0));
-    // E21 = -S^{-1} W ; E11 = A^{-1} - W^T E21 ; E22 = S^{-1}
-    const double e20 = -fma(j00, w00, j01 * w10), e21 = -fma(j00, w01, j01 * w11);
-    const double e30 = -fma(j01, w00, j11 * w10), e31 = -fma(j01, w01, j11 * w11);
-    const double e00 = i00 - fma(w00, e20, w10 * e30);
-    const double e01 = i01 - fma(w00, e21, w10 * e31);
-    const double e11 = i11 - fma(w01, e21, w11 * e31);
-    // store F = -E (symmetric)
-    d[0][0] = -e00; d[0][1] = d[1][0] = -e01; d[1][1] = -e11;
-    d[2][0] = d[0][2] = -e20; d[2][1] = d[1][2] = -e21;
-    d[3][0] = d[0][3] = -e30; d[3][1] = d[1][3] = -e31;
-    d[2][2] = -j00; d[3][2] = d[2][3] = -j01; d[3][3] = -j11;
-}
-
-__device__ __forceinline__ double sel4(const double (&v)[4], int i)
-{
-    double x = v[0];
-    x = (i == 1) ? v[1] : x;
-    x = (i == 2) ? v[2] : x;
-    x = (i == 3) ? v[3] : x;
-    return x;
+    double l[4][4], rd[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double dk = d[k][k];
+        flags |= pivot_flags(dk);
+        cnt += (dk < 0.0);
+        const double rk = pivot_reciprocal(dk);
+        rd[k] = rk;
+#pragma unroll
+        for (int i = k + 1; i < 4; ++i) l[i][k] = d[i][k] * rk;
+#pragma unroll
+        for (int i = k + 1; i < 4; ++i)
+#pragma unroll
+            for (int j = k + 1; j <= i; ++j) d[i][j] = fma(-l[i][k], d[j][k], d[i][j]);
+    }
+    // Lam = L^{-1} by forward substitution
+    double lam[4][4];
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < i; ++j) {
+            double s = -l[i][j];
+#pragma unroll
+            for (int m = j + 1; m < i; ++m) s = fma(-l[i][m], lam[m][j], s);
+            lam[i][j] = s;
+        }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) d[i][j] = (i == j) ? rd[i] : (i > j ? lam[i][j] : 0.0);
 }
 
 // Gather the 4x4 pivot block rows/cols 4H..4H+3 of diagonal tile (K, K)
-// into every lane with shuffles: element (i, j) sits in lane
-// (4H+i)*4 + 2H + (j>>1), slot j&1.  Symmetric, so ten shuffles.
+// into every lane with shuffles, lower triangle only: element (i, j), i >= j,
+// sits in lane (4H+i)*4 + 2H + (j>>1), slot j&1.  Ten shuffles.
 template <int NT, int K, int H>
 __device__ __forceinline__ void gather_block(const double (&a)[G<NT>::NTL][2], int lane, double (&f)[4][4])
 {
@@ -113,31 +110,50 @@ __device__ __forceinline__ void gather_block(const double (&a)[G<NT>::NTL][2], i
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = i; j < 4; ++j) {
+        for (int j = 0; j <= i; ++j) {
             const int src = (4 * H + i) * 4 + 2 * H + (j >> 1);
-            const double v = __shfl_sync(0xffffffffu, a[tix(K, K)][j & 1], src);
-            f[i][j] = v;
-            f[j][i] = v;
+            f[i][j] = __shfl_sync(0xffffffffu, a[tix(K, K)][j & 1], src);
         }
 }
 
+// This lane's share of the block operands (ldl_block4 layout in f): row q of
+// Lam below the diagonal (lq[m], m < q; zero for m >= q) and 1/delta_q.
+__device__ __forceinline__ void lane_operands(const double (&f)[4][4], int q, double (&lq)[3], double &rq)
+{
+    lq[0] = (q == 1) ? f[1][0] : (q == 2) ? f[2][0] : (q == 3) ? f[3][0] : 0.0;
+    lq[1] = (q == 2) ? f[2][1] : (q == 3) ? f[3][1] : 0.0;
+    lq[2] = (q == 3) ? f[3][2] : 0.0;
+    rq = (q == 1) ? f[1][1] : (q == 2) ? f[2][2] : (q == 3) ? f[3][3] : f[0][0];
+}
+
+// Lam[q][a] from this lane's row of Lam
+__device__ __forceinline__ double lam_qa(const double (&lq)[3], int q, int a)
+{
+    const double x = (a == 0) ? lq[0] : (a == 1) ? lq[1] : (a == 2) ? lq[2] : 0.0;
+    return (a == q) ? 1.0 : x;
+}
+
 // One block of four pivots, tile column K, half H (p0 = 8K + 4H).  f holds
-// F = -D^{-1} of this block on entry and the next block's on exit (computed
-// right after the next block's diagonal tile is updated, so its latency
-// overlaps the rest of this block's DMMAs).
+// the block's operands (ldl_block4) on entry and the next block's on exit
+// (computed right after the next block's diagonal tile is updated, so its
+// latency overlaps the rest of this block's DMMAs).
 template <int NT, int K, int H>
-__device__ __forceinline__ void sweep_round(double (&a)[G<NT>::NTL][2], double *__restrict__ pan, int n,
+__device__ __forceinline__ void sweep_round(double (&a)[G<NT>::NTL][2], double *pan, int n,
                                             int lane, double (&f)[4][4], int &cnt, int &flags)
 {
     const int r = lane >> 2, q = lane & 3;
     constexpr int K2 = H ? K + 1 : K;  // next block
     constexpr int H2 = H ? 0 : 1;
     constexpr int p2 = 8 * K2 + 4 * H2;  // first pivot of the next block
-    // publish the panel A[:, P] (row i -> pan[4i .. 4i+3])
+    // publish the panel A[i, P] (row i -> pan[4i .. 4i+3]) from the lower
+    // triangle: tiles below the diagonal in tile column K directly, tiles left
+    // of it in tile row K transposed; in diagonal tile K the rows of the other
+    // half come from whichever side of it lies in the lower triangle (rows of
+    // P themselves are not needed)
     __syncwarp();
     if ((q >> 1) == H) {
 #pragma unroll
-        for (int I = K; I < NT; ++I) {
+        for (int I = (H ? K + 1 : K); I < NT; ++I) {
             pan[(8 * I + r) * 4 + 2 * q - 4 * H] = a[tix(I, K)][0];
             pan[(8 * I + r) * 4 + 2 * q - 4 * H + 1] = a[tix(I, K)][1];
         }
@@ -148,17 +164,15 @@ __device__ __forceinline__ void sweep_round(double (&a)[G<NT>::NTL][2], double *
             pan[(8 * J + 2 * q) * 4 + (r & 3)] = a[tix(K, J)][0];
             pan[(8 * J + 2 * q + 1) * 4 + (r & 3)] = a[tix(K, J)][1];
         }
+        if (H == 1 && q < 2) {
+            pan[(8 * K + 2 * q) * 4 + (r & 3)] = a[tix(K, K)][0];
+            pan[(8 * K + 2 * q + 1) * 4 + (r & 3)] = a[tix(K, K)][1];
+        }
     }
     __syncwarp();
-    double fq[4];  // column q of F
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        double x = f[m][0];
-        x = (q == 1) ? f[m][1] : x;
-        x = (q == 2) ? f[m][2] : x;
-        x = (q == 3) ? f[m][3] : x;
-        fq[m] = x;
-    }
+    double lq[3], rq;
+    lane_operands(f, q, lq, rq);
+    const double nrq = -rq;
     // zero row/column block P
 #pragma unroll
     for (int I = K; I < NT; ++I) {
@@ -175,23 +189,27 @@ __device__ __forceinline__ void sweep_round(double (&a)[G<NT>::NTL][2], double *
 #pragma unroll
     for (int I = 0; I < NT; ++I) {
         const double2 *row = reinterpret_cast<const double2 *>(pan + (8 * I + r) * 4);
-        const double2 x01 = row[0], x23 = row[1];
-        X[I] = fma(x01.x, fq[0], fma(x01.y, fq[1], fma(x23.x, fq[2], x23.y * fq[3])));
-        B[I] = pan[(8 * I + r) * 4 + q];
+        const double2 x01 = row[0];
+        const double x2 = row[1].x;
+        const double vq = pan[(8 * I + r) * 4 + q];
+        const double c = fma(lq[0], x01.x, fma(lq[1], x01.y, fma(lq[2], x2, vq)));
+        X[I] = c * nrq;
+        B[I] = c;
     }
     if ((r >> 2) == H) {
-        // rows of P: X = -F ; columns of P: B = -I
-        X[K] = -sel4(fq, r & 3);
-        B[K] = (q == (r & 3)) ? -1.0 : 0.0;
+        // rows of P: X = Lam[q][a] / delta_q , B = -Lam[q][a]  (a = r & 3)
+        const double la = lam_qa(lq, q, r & 3);
+        X[K] = la * rq;
+        B[K] = -la;
     }
-    // The next block's diagonal tile first; its F is computed while the other
-    // DMMAs run.  Then the rest of the next panel's tile column and row, so
-    // the next round can publish early; the remaining tiles last.
+    // The next block's diagonal tile first; its operands are formed while the
+    // other DMMAs run.  Then the rest of the next panel's tile column and row,
+    // so the next round can publish early; the remaining tiles last.
     if (K2 < NT) {
         constexpr int KG = K2 < NT ? K2 : 0;
         dmma(a[tix(KG, KG)][0], a[tix(KG, KG)][1], X[KG], B[KG]);
         gather_block<NT, KG, H2>(a, lane, f);
-        neg_inverse4(f, n - p2, cnt, flags);  // n - p2 <= 0: all padding, counts nothing
+        ldl_block4(f, n - p2, cnt, flags);  // n - p2 <= 0: all padding, counts nothing
 #pragma unroll
         for (int I = KG + 1; I < NT; ++I) dmma(a[tix(I, KG)][0], a[tix(I, KG)][1], X[I], B[KG]);
 #pragma unroll
@@ -230,7 +248,7 @@ __device__ __forceinline__ int warp_sweep_invert(double (&a)[G<NT>::NTL][2], dou
     int cnt = 0, flags = 0;
     double f[4][4];
     gather_block<NT, 0, 0>(a, lane, f);
-    neg_inverse4(f, n, cnt, flags);
+    ldl_block4(f, n, cnt, flags);
     Rounds<NT, 0>::run(a, pan, n, lane, f, cnt, flags);
     bad = flags_to_status(flags);
     return cnt;

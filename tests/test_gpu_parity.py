@@ -41,15 +41,35 @@ def oracle_prop(prop, c, seg, ered, y0):
 
 
 @pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 12, 17, 30, 31, 36, 45, 64])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 12, 17, 30, 31, 36, 40, 41, 45, 64, 80, 100, 128, 150, 200])
 def test_random_systems(prop, n):
-    c, seg, ered, y0 = cases.random_case(n, 160, seed=1000 + n)
+    """One warp per matrix (N <= 40), one CTA per matrix (N <= 200; LDPROP
+    <= 128), all on FP64 tensor cores."""
+    if prop == "LDJ" and n > 128:
+        pytest.skip("LDPROP keeps two matrices in shared memory: N <= 128")
+    nstep = 160 if n <= 64 else 60
+    c, seg, ered, y0 = cases.random_case(n, nstep, seed=1000 + n)
     yg, ng = propagate(prop, c, seg, ered, y0)
     yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
     assert st == 0
     assert ng == no
     assert cases.rel_err(yg, yo) < Y_TOL
     assert np.array_equal(yg, yg.T)
+
+
+@pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
+@pytest.mark.parametrize("n", [3, 17, 36, 45, 64])
+def test_register_tile_family(prop, n):
+    """The 4x4 register-tile kernels (scalar sweep) selected explicitly."""
+    old = _lib.set_kernel_family(_lib.FAMILY_TILE4)
+    try:
+        c, seg, ered, y0 = cases.random_case(n, 160, seed=2000 + n)
+        yg, ng = propagate(prop, c, seg, ered, y0)
+    finally:
+        _lib.set_kernel_family(old)
+    yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
+    assert st == 0 and ng == no
+    assert cases.rel_err(yg, yo) < Y_TOL
 
 
 @pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
@@ -120,7 +140,7 @@ def test_rotor_full_grid(jtot, block, n):
 def test_batch_equals_alone():
     """Every job of a mixed batch (several N buckets, energies, both
     propagators' systems) gives exactly the result it gives alone."""
-    items = [cases.random_case(n, 120, seed=500 + n) for n in (3, 9, 16, 30, 33)]
+    items = [cases.random_case(n, 120, seed=500 + n) for n in (3, 9, 16, 30, 33, 47, 90)]
     systems = [it[0] for it in items]
     segs = [it[1] for it in items]
     job_sys, job_e, y0s = [], [], []
@@ -177,9 +197,9 @@ def test_nonfinite_potential_is_flagged():
 
 
 def test_unsupported_size():
-    n = _lib.load().mgpu_max_n() + 1
-    c = Coupling(n=n, nham=1, vl=np.zeros(n * (n + 1) // 2), eint=np.zeros(n), cent=np.zeros(n))
-    seg = Segment(1, 0.1, np.array([1.0, 1.05, 1.1]), np.zeros((3, 1)))
-    with pytest.raises(PropagatorError) as e:
-        propagate("LDMD", c, seg, 1.0, np.eye(n))
-    assert e.value.status == _lib.MGPU_ERR_UNSUPPORTED
+    for prop, n in (("LDMD", _lib.load().mgpu_max_n() + 1), ("LDJ", 129)):
+        c = Coupling(n=n, nham=1, vl=np.zeros(n * (n + 1) // 2), eint=np.zeros(n), cent=np.zeros(n))
+        seg = Segment(1, 0.1, np.array([1.0, 1.05, 1.1]), np.zeros((3, 1)))
+        with pytest.raises(PropagatorError) as e:
+            propagate(prop, c, seg, 1.0, np.eye(n))
+        assert e.value.status == _lib.MGPU_ERR_UNSUPPORTED
