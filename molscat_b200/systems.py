@@ -189,11 +189,10 @@ class Workload:
         return float(sum(self.systems[s].n ** 3 * self.segments[s].nstep for s in self.job_sys))
 
 
-def _rotor_jobs(jtots, blocks, energies_cm, name):
+def _rotor_jobs(jtots, blocks, energies_cm, name, nstep=ROTOR_NSTEP):
     sysm = rotor_system()
     rmin = ROTOR_RMIN_A / sysm.rm
     rmax = ROTOR_RMAX_A / sysm.rm
-    nstep = ROTOR_NSTEP
     dr = (rmax - rmin) / nstep
     systems, segments, labels = [], [], []
     job_sys, job_ered, job_y0 = [], [], []
@@ -227,8 +226,10 @@ def batched_energies(count: int = 512, seed: int = 20261203) -> np.ndarray:
     return np.random.default_rng(seed).uniform(1.0, 500.0, size=count)
 
 
-def batched_workload(n_energies: int = 512, jmax: int = 80, seed: int = 20261203, jtots=None) -> Workload:
+def batched_workload(n_energies: int = 512, jmax: int = 80, seed: int = 20261203, jtots=None,
+                     nstep: int = ROTOR_NSTEP) -> Workload:
     """JTOT=0..jmax, both parity blocks, n_energies seeded energies."""
     jt = list(range(0, jmax + 1)) if jtots is None else list(jtots)
     e = batched_energies(n_energies, seed)
-    return _rotor_jobs(jt, [1, 2], e, f"rotor JTOT=0..{jmax} x 2 parities x {n_energies} energies, 4000 steps")
+    return _rotor_jobs(jt, [1, 2], e, f"rotor JTOT=0..{jmax} x 2 parities x {n_energies} energies, {nstep} steps",
+                       nstep=nstep)
