@@ -157,7 +157,8 @@ int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_
  * Instead of allocating, the library uses one fixed 64 MiB scratch array,
  * reserved on every GPU that loads the library until the process exits.  A
  * request that needs more (about 128*NSTEP*NT*(NT+1)/2 bytes for the per-step
- * 2HQ(C) table, NT = ceil(N/4)) or more than 4096 jobs is rejected with
+ * 2HQ(C) table, NT = ceil(N/4)), more than 4096 jobs or N above 200 (the
+ * large-N kernels need per-job device matrices) is rejected with
  * MGPU_ERR_UNSUPPORTED.  All calls share that array and it keeps the last
  * call's contents (each call rewrites what it reads and zeroes its counters),
  * so calls that overlap on the GPU -- on different streams or from different
@@ -177,7 +178,7 @@ int mgpu_set_kernel_family(int family);
 /* ---- diagnostics --------------------------------------------------------- */
 const char *mgpu_status_string(int status);
 const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */
-int mgpu_max_n(void);                /* largest N MDPROP accepts (LDPROP: 128) */
+int mgpu_max_n(void);                /* largest N the propagators accept (1024) */
 
 #ifdef __cplusplus
 }

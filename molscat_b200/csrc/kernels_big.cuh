@@ -1,0 +1,534 @@
+// LDMD / LDJ for large N (NPAD = 64*m, 256 <= NPAD <= 1024): the matrices of
+// a batch live in global memory (L2 / HBM) as lower 8x8 tiles in the DMMA
+// accumulator layout of warp_dmma.cuh (tile t = I(I+1)/2 + J, lane l holds
+// (8I + l/4, 8J + 2(l%4) + s)).  Included by propagator.cu after
+// kernels_cta.cuh.
+//
+// Inversion is the symmetric Gauss-Jordan sweep of warp_dmma.cuh with 64
+// pivots a round (one tile row/column block P of 8 tiles), in three batched
+// kernels per round over all matrices of the batch:
+//   factor  one CTA per matrix: unpivoted LDL^T of D = A_PP (lower triangle
+//           only), Lam = L^{-1} and 1/delta_k, negative pivots counted
+//           (SYMINV's KOUNT, syminv.f:27-49);
+//   panel   every 8-row block: c = A[i, P] Lam^T on DMMA, written as the
+//           update operands X = -c/delta, B = c (rows of P: X = Lam^T/delta,
+//           B = -Lam^T) in A-fragment order;
+//   update  every lower tile: tiles of row/column block P zeroed, then
+//           A_IJ += X_I B_J^T on DMMA (64 k-steps of m8n8k4), X and B staged
+//           in shared memory by bulk (TMA) copies.
+// which leaves A_ij - sum_k c_k(i) c_k(j)/delta_k outside P, A_iP D^{-1} in
+// the columns of P and -D^{-1} in A_PP, the scalar sweep's values.  All reads
+// take the lower triangle, so rounding left in the upper halves of diagonal
+// tiles never feeds back.
+//
+// The step's elementwise parts (HAMMAT W, the reference-potential solutions,
+// the Y updates of mdprop.f / ldprop.f) are separate batched kernels; a
+// device-side step counter lets one step's launch sequence repeat unchanged.
+#pragma once
+#include "kernels_cta.cuh"
+
+namespace mgpu {
+namespace big {
+
+using wf::tix;
+
+constexpr int NB = 64;      // pivots per round
+constexpr int KB = NB / 8;  // tile columns per round
+constexpr int MC = NB / 4;  // m8n8k4 k-steps per round
+constexpr int FACT_THREADS = 256;
+constexpr int PANEL_WARPS = 8;
+constexpr int UPD_WARPS = 4;
+constexpr int EW_THREADS = 256;
+constexpr int kBigMaxNT = 128;  // NPAD <= 1024
+
+// One matrix of an inversion batch.
+struct MatDesc {
+    double *a;   // lower tiles, NT(NT+1)/2 * 64 doubles
+    int *cnt;    // negative-pivot counter, incremented by sign * count
+    int *stat;   // failure status (atomicMax)
+    int *kfail;  // step of the first failure (atomicMin)
+    int n;       // channels; rows >= n are padding (zero, unit pivot)
+    int sign;    // +1 or -1
+    int nstep;   // the matrix takes part while the step counter is <= nstep
+    int kfix;    // > 0: report this step on failure instead of the counter
+};
+
+// Per-matrix scratch of one round.
+struct Panels {
+    double *lam;  // [M][64*64] Lam row-major
+    double *rd;   // [M][64] 1/delta
+    double *xf;   // [M][NT][MC][32] X in A-fragment order
+    double *bf;   // [M][NT][MC][32] B in A-fragment order
+};
+
+__device__ __forceinline__ size_t sym_index(int i, int j)
+{
+    const int R = i > j ? i : j, C = i > j ? j : i;
+    return (size_t)tix(R >> 3, C >> 3) * 64 + ((R & 7) * 4 + ((C & 7) >> 1)) * 2 + (C & 1);
+}
+
+// tile t -> (I, J), I >= J
+__device__ __forceinline__ void tile_ij(int t, int &I, int &J)
+{
+    int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while (i * (i + 1) / 2 > t) --i;
+    while ((i + 1) * (i + 2) / 2 <= t) ++i;
+    I = i;
+    J = t - i * (i + 1) / 2;
+}
+
+// element x of a tiled matrix -> (row, column)
+__device__ __forceinline__ void elem_ij(size_t x, int &i, int &j)
+{
+    int I, J;
+    tile_ij((int)(x >> 6), I, J);
+    const int l = (int)(x >> 1) & 31, s = (int)x & 1;
+    i = 8 * I + (l >> 2);
+    j = 8 * J + 2 * (l & 3) + s;
+}
+
+__device__ __forceinline__ void report_failure(const MatDesc &md, int flags, int k)
+{
+    const int code = (flags & 1) ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+    atomicMax(md.stat, code);
+    atomicMin(md.kfail, md.kfix > 0 ? md.kfix : k);
+}
+
+// ---------------------------------------------------------------------------
+// factor: LDL^T of the 64x64 pivot block, Lam = L^{-1}, 1/delta
+// ---------------------------------------------------------------------------
+constexpr size_t kFactSmem = 2 * (size_t)NB * (NB + 1) * sizeof(double);  // D and Lam, padded rows
+
+__global__ void __launch_bounds__(FACT_THREADS)
+big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const int *__restrict__ kstep)
+{
+    extern __shared__ __align__(16) double fsm[];
+    double (*D)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm);
+    double (*L)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm + NB * (NB + 1));
+    __shared__ int s_cnt, s_flags;
+    const MatDesc md = mds[blockIdx.x];
+    const int k = *kstep;
+    if (k > md.nstep) return;
+    const int p0 = NB * round, K0 = KB * round;
+    const int tid = threadIdx.x;
+    for (int x = tid; x < NB * NB; x += FACT_THREADS) {
+        const int i = x >> 6, j = x & 63;
+        double v = 0.0;
+        if (j <= i) v = md.a[(size_t)tix(K0 + (i >> 3), K0 + (j >> 3)) * 64 + ((i & 7) * 4 + ((j & 7) >> 1)) * 2 + (j & 1)];
+        if (i == j && p0 + i >= md.n) v = 1.0;  // padding pivot
+        D[i][j] = v;
+        L[i][j] = (i == j) ? 1.0 : 0.0;
+    }
+    if (tid == 0) s_cnt = s_flags = 0;
+    // thread -> row i, columns j = c0 (mod 4)
+    const int i = tid >> 2, c0 = tid & 3;
+    for (int kk = 0; kk < NB; ++kk) {
+        __syncthreads();
+        const double dk = D[kk][kk];
+        const double rk = pivot_reciprocal(dk);
+        if (tid == 0) {
+            if (p0 + kk < md.n && dk < 0.0) ++s_cnt;
+            s_flags |= pivot_flags(dk);
+        }
+        if (i > kk) {
+            const double li = D[i][kk] * rk;
+            for (int j = kk + 1 + ((c0 - kk - 1) & 3); j <= i; j += 4) D[i][j] = fma(-li, D[j][kk], D[i][j]);
+            for (int c = c0; c <= kk; c += 4) L[i][c] = fma(-li, L[kk][c], L[i][c]);
+        }
+    }
+    __syncthreads();
+    double *lam = pn.lam + (size_t)blockIdx.x * NB * NB;
+    for (int x = tid; x < NB * NB; x += FACT_THREADS) lam[x] = L[x >> 6][x & 63];
+    if (tid < NB) pn.rd[(size_t)blockIdx.x * NB + tid] = pivot_reciprocal(D[tid][tid]);
+    if (tid == 0) {
+        if (s_cnt) atomicAdd(md.cnt, md.sign * s_cnt);
+        if (s_flags) report_failure(md, s_flags, k);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// panel: operand rows X, B of every 8-row block (one warp each)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(32 * PANEL_WARPS)
+big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep)
+{
+    __shared__ __align__(16) double lamB[KB][MC][32];
+    __shared__ double s_r[NB];
+    const int m = blockIdx.y;
+    const MatDesc md = mds[m];
+    if (*kstep > md.nstep) return;
+    const double *lam = pn.lam + (size_t)m * NB * NB;
+    // B fragments of Lam^T: (k-row q, column r) of output tile kt, k-step mc
+    for (int x = threadIdx.x; x < KB * MC * 32; x += blockDim.x) {
+        const int ln = x & 31, mc = (x >> 5) % MC, kt = x / (32 * MC);
+        lamB[kt][mc][ln] = lam[(8 * kt + (ln >> 2)) * NB + 4 * mc + (ln & 3)];
+    }
+    if (threadIdx.x < NB) s_r[threadIdx.x] = pn.rd[(size_t)m * NB + threadIdx.x];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3;
+    const int I = blockIdx.x * PANEL_WARPS + warp;
+    if (I >= nt) return;
+    const int p0 = NB * round, K0 = KB * round;
+    double *xf = pn.xf + ((size_t)m * nt + I) * MC * 32;
+    double *bf = pn.bf + ((size_t)m * nt + I) * MC * 32;
+    if (I >= K0 && I < K0 + KB) {
+        // rows of P: X(p0+a, k) = Lam[k][a] / delta_k, B(p0+a, k) = -Lam[k][a]
+        const int a = 8 * (I - K0) + r;
+        for (int mc = 0; mc < MC; ++mc) {
+            const int kk = 4 * mc + q;
+            const double la = lam[kk * NB + a];
+            xf[mc * 32 + lane] = la * s_r[kk];
+            bf[mc * 32 + lane] = -la;
+        }
+        return;
+    }
+    double acc[KB][2];
+#pragma unroll
+    for (int kt = 0; kt < KB; ++kt) acc[kt][0] = acc[kt][1] = 0.0;
+    const int i = 8 * I + r;
+#pragma unroll 4
+    for (int mc = 0; mc < MC; ++mc) {
+        const double v = md.a[sym_index(i, p0 + 4 * mc + q)];  // A[i, p0 + 4mc + q] (A fragment)
+#pragma unroll
+        for (int kt = 0; kt < KB; ++kt) wf::dmma(acc[kt][0], acc[kt][1], v, lamB[kt][mc][lane]);
+    }
+    // acc[kt][s] = c(8I + r, 8kt + 2q + s) -> A-fragment slot (k-step 2kt + q/2, lane r*4 + 2(q&1) + s)
+#pragma unroll
+    for (int kt = 0; kt < KB; ++kt) {
+        const int col = 8 * kt + 2 * q;
+        const int o = (2 * kt + (q >> 1)) * 32 + r * 4 + 2 * (q & 1);
+        *reinterpret_cast<double2 *>(bf + o) = make_double2(acc[kt][0], acc[kt][1]);
+        *reinterpret_cast<double2 *>(xf + o) = make_double2(acc[kt][0] * -s_r[col], acc[kt][1] * -s_r[col + 1]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// update: A_IJ = [IJ outside P] A_IJ + X_I B_J^T over a block of 8x8 tiles
+// ---------------------------------------------------------------------------
+constexpr uint32_t kUpdHalfBytes = KB * MC * 32 * sizeof(double);  // 32 KB: 8 tile rows of X (or B)
+constexpr size_t kUpdSmem = 2 * (size_t)kUpdHalfBytes;
+
+__global__ void __launch_bounds__(32 * UPD_WARPS)
+big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep)
+{
+    extern __shared__ __align__(128) double usm[];
+    __shared__ __align__(8) uint64_t bar;
+    const int m = blockIdx.y;
+    const MatDesc md = mds[m];
+    if (*kstep > md.nstep) return;
+    int BI, BJ;
+    tile_ij(blockIdx.x, BI, BJ);
+    double *Xs = usm, *Bs = usm + KB * MC * 32;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 2);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bulk_load(Xs, pn.xf + ((size_t)m * nt + 8 * BI) * MC * 32, kUpdHalfBytes, &bar);
+        bulk_load(Bs, pn.bf + ((size_t)m * nt + 8 * BJ) * MC * 32, kUpdHalfBytes, &bar);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool inP = (BI == round) || (BJ == round);  // whole tiles of row/column block P
+    const int I0 = 8 * BI + 2 * warp;
+    double acc[2][KB][2];
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jt = 0; jt < KB; ++jt) {
+            const int I = I0 + ii, J = 8 * BJ + jt;
+            double2 c = make_double2(0.0, 0.0);
+            if (I >= J && !inP) c = *reinterpret_cast<const double2 *>(md.a + (size_t)tix(I, J) * 64 + lane * 2);
+            acc[ii][jt][0] = c.x;
+            acc[ii][jt][1] = c.y;
+        }
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (threadIdx.x == 0) atomicMax(md.stat, MGPU_ERR_TIMEOUT);
+        mbar_wait_bounded(&bar, 0);  // let the copies land before the CTA's shared memory goes
+        return;
+    }
+    const double *xa = Xs + (2 * warp) * MC * 32 + lane;
+#pragma unroll 2
+    for (int mc = 0; mc < MC; ++mc) {
+        const double a0 = xa[mc * 32], a1 = xa[MC * 32 + mc * 32];
+#pragma unroll
+        for (int jt = 0; jt < KB; ++jt) {
+            const double b = Bs[(jt * MC + mc) * 32 + lane];
+            const int J = 8 * BJ + jt;
+            if (I0 >= J) wf::dmma(acc[0][jt][0], acc[0][jt][1], a0, b);
+            if (I0 + 1 >= J) wf::dmma(acc[1][jt][0], acc[1][jt][1], a1, b);
+        }
+    }
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+        for (int jt = 0; jt < KB; ++jt) {
+            const int I = I0 + ii, J = 8 * BJ + jt;
+            if (I >= J)
+                *reinterpret_cast<double2 *>(md.a + (size_t)tix(I, J) * 64 + lane * 2) =
+                    make_double2(acc[ii][jt][0], acc[ii][jt][1]);
+        }
+}
+
+// ---------------------------------------------------------------------------
+// elementwise parts of a step (one job per blockIdx.y)
+// ---------------------------------------------------------------------------
+struct StepArgs {
+    const SysDev *sys;
+    const JobDev *jobs;
+    const MatDesc *md;    // per job: its (Z) matrix, counters and status
+    double *tiles2;       // LDJ: U matrices, [M][TD]
+    double *vec;          // LDMD: [M][3][NPAD] y14, y14' = y14 - D1 W_ii, y23
+    const int *kstep;
+    int npad;
+    size_t td;            // doubles of one tiled matrix
+};
+
+__device__ __forceinline__ const double *ptab_row(const SysDev &S, int ir) { return S.ptab + (size_t)ir * S.nham; }
+
+// MDPROP start: Y tiles = H Y0 + D1 W(RSTART) (mdprop.f:89-93); counters reset
+__global__ void __launch_bounds__(EW_THREADS) big_ldmd_init_kernel(StepArgs a, const double *__restrict__ y)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *md.cnt = 0;
+        *md.stat = S.prep[1];  // a failed preparation fails every job of the system
+        *md.kfail = S.prep[1] ? S.prep[2] : INT_MAX;
+    }
+    const double h = S.dr / 2.0, d1 = h * h / 3.0;
+    const double *yj = y + job.yoff;
+    const int n = S.n;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        const double y0 = (i < n && j < n) ? yj[(size_t)lo * n + hi] : 0.0;
+        md.a[x] = h * y0 + d1 * cta::w_elem(S, ptab_row(S, 0), (int)x, i, j, 0, job.ered, true);
+    }
+}
+
+// reference-potential solutions of step k and Y += y14' on the diagonal (mdprop.f:143-164)
+__global__ void __launch_bounds__(EW_THREADS) big_ldmd_pre_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int k = *a.kstep;
+    if (k > md.nstep) return;
+    const int i = blockIdx.x * EW_THREADS + threadIdx.x;
+    if (i >= a.npad) return;
+    double *v = a.vec + (size_t)m * 3 * a.npad;
+    double y14 = 0.0, y14b = 0.0, y23 = 0.0;
+    if (i < S.n) {
+        const double h = S.dr / 2.0, d1 = h * h / 3.0;
+        const int ir = 2 * k - 1;
+        const size_t e = (size_t)tix(i >> 3, i >> 3) * 64 + ((i & 7) * 4 + ((i & 7) >> 1)) * 2 + (i & 1);
+        const double wref = cta::w_elem(S, ptab_row(S, ir), (int)e, i, i, ir, job.ered, true);
+        ref_solutions(wref, 0.5 * h, y14, y23);
+        y14b = y14 - d1 * wref;
+        md.a[e] += y14b;
+    }
+    v[i] = y14;
+    v[a.npad + i] = y14b;
+    v[2 * a.npad + i] = y23;
+}
+
+// Y = 2HQ(C_k) + 2 Y14 - Y23 Y^-1 Y23  (tiles hold -Y^-1; mdprop.f:156,181-185)
+__global__ void __launch_bounds__(EW_THREADS) big_ldmd_mid_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int k = *a.kstep;
+    if (k > md.nstep) return;
+    const double *v = a.vec + (size_t)m * 3 * a.npad;
+    const double *qk = S.q + (size_t)(k - 1) * a.td;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        double w = __ldg(qk + x) + v[2 * a.npad + i] * md.a[x] * v[2 * a.npad + j];
+        if (i == j) w += 2.0 * v[i];
+        md.a[x] = w;
+    }
+}
+
+// Y = D2 W(B) - Y23 Y^-1 Y23 + Y14' (D1 at the last step; mdprop.f:196-230)
+__global__ void __launch_bounds__(EW_THREADS) big_ldmd_post_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int k = *a.kstep;
+    if (k > md.nstep) return;
+    const double h = S.dr / 2.0, d1 = h * h / 3.0, d2 = 2.0 * d1;
+    const double dd = (k == S.nstep) ? d1 : d2;
+    const double *v = a.vec + (size_t)m * 3 * a.npad;
+    const double *P = ptab_row(S, 2 * k);
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        double w = dd * cta::w_elem(S, P, (int)x, i, j, 2 * k, job.ered, true) + v[2 * a.npad + i] * md.a[x] * v[2 * a.npad + j];
+        if (i == j) w += v[a.npad + i];
+        md.a[x] = w;
+    }
+}
+
+// LDPROP start: Z = H Y0 + D1 W(RSTART) + I (ldprop.f:30-44)
+__global__ void __launch_bounds__(EW_THREADS) big_ldj_init_kernel(StepArgs a, const double *__restrict__ y)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *md.cnt = 0;
+        *md.stat = 0;
+        *md.kfail = INT_MAX;
+    }
+    const double h = S.dr / 2.0, d1 = h * h / 3.0;
+    const double *yj = y + job.yoff;
+    const int n = S.n;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        const double y0 = (i < n && j < n) ? yj[(size_t)lo * n + hi] : 0.0;
+        md.a[x] = h * y0 + d1 * cta::w_elem(S, ptab_row(S, 0), (int)x, i, j, 0, job.ered, true) +
+                  ((i == j && i < n) ? 1.0 : 0.0);
+    }
+}
+
+// U(C) = I/8 + D4 W(C) (ldprop.f:60-76)
+__global__ void __launch_bounds__(EW_THREADS) big_ldj_pre_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int k = *a.kstep;
+    if (k > md.nstep) return;
+    const double h = S.dr / 2.0, d4 = -h * h / 48.0;
+    double *u = a.tiles2 + (size_t)m * a.td;
+    const double *P = ptab_row(S, 2 * k - 1);
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        u[x] = d4 * cta::w_elem(S, P, (int)x, i, j, 2 * k - 1, job.ered, true) + ((i == j && i < S.n) ? 0.125 : 0.0);
+    }
+}
+
+// Z = -U^-1 ... : Z <- (-U^{-1}) + (-Z^{-1}) - 6I in the sweep's signs (ldprop.f:92-97)
+__global__ void __launch_bounds__(EW_THREADS) big_ldj_mid_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    if (*a.kstep > md.nstep) return;
+    const double *u = a.tiles2 + (size_t)m * a.td;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        md.a[x] = -u[x] + md.a[x] - ((i == j && i < S.n) ? 6.0 : 0.0);
+    }
+}
+
+// Z = D2 W(B) + 2I + Z (D1 at the last step; ldprop.f:103-126)
+__global__ void __launch_bounds__(EW_THREADS) big_ldj_post_kernel(StepArgs a)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int k = *a.kstep;
+    if (k > md.nstep) return;
+    const double h = S.dr / 2.0, d1 = h * h / 3.0, d2 = 2.0 * d1;
+    const double dd = (k == S.nstep) ? d1 : d2;
+    const double *P = ptab_row(S, 2 * k);
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        md.a[x] = dd * cta::w_elem(S, P, (int)x, i, j, 2 * k, job.ered, true) + ((i == j && i < S.n) ? 2.0 : 0.0) +
+                  md.a[x];
+    }
+}
+
+// Results: Y = tiles/H (MDPROP, mdprop.f:269-275) or Z/H - I/H (LDPROP,
+// ldprop.f:140-147) into the caller's column-major Y, both triangles;
+// NODES (MDPROP: minus the U(C) count NSAVE), status and failing step.
+__global__ void __launch_bounds__(EW_THREADS)
+big_finish_kernel(StepArgs a, int ldj, double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                  int *__restrict__ kfail_out)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev &S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int st = *md.stat;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        status_out[job.out] = st;
+        kfail_out[job.out] = st ? *md.kfail : 0;
+        nodes_out[job.out] = st ? 0 : (*md.cnt - (ldj ? 0 : S.prep[0]));
+    }
+    if (st) return;
+    const double hi = 2.0 / S.dr;
+    const int n = S.n;
+    double *yj = y + job.yoff;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        if (i < n && j <= i) {
+            const double v = hi * md.a[x] - ((ldj && i == j) ? hi : 0.0);
+            yj[(size_t)j * n + i] = v;
+            yj[(size_t)i * n + j] = v;
+        }
+    }
+}
+
+__global__ void big_step_advance_kernel(int *kstep, int value)
+{
+    if (value >= 0) *kstep = value;
+    else ++*kstep;
+}
+
+// ---------------------------------------------------------------------------
+// MDPROP preparation: U(C_k) = I/8 - (H^2/48) W_off(C_k) for a range of steps
+// of one system, inverted in place as a batch, then 2HQ(C_k) = U^{-1} - 8I
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(EW_THREADS) big_prep_build_kernel(const SysDev *__restrict__ sys, int s, int k0, size_t td)
+{
+    const SysDev &S = sys[s];
+    const int k = k0 + blockIdx.y;
+    if (k > S.nstep) return;
+    const double h = S.dr / 2.0, d4 = -h * h / 48.0;
+    double *u = S.q + (size_t)(k - 1) * td;
+    const double *P = ptab_row(S, 2 * k - 1);
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        u[x] = (i == j) ? (i < S.n ? 0.125 : 0.0) : d4 * cta::w_elem(S, P, (int)x, i, j, 2 * k - 1, 0.0, false);
+    }
+}
+
+__global__ void __launch_bounds__(EW_THREADS) big_prep_finish_kernel(const SysDev *__restrict__ sys, int s, int k0, size_t td)
+{
+    const SysDev &S = sys[s];
+    const int k = k0 + blockIdx.y;
+    if (k > S.nstep) return;
+    double *u = S.q + (size_t)(k - 1) * td;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        // tiles = -U^{-1};  2HQ(C) = U^{-1} - 8I
+        u[x] = (i >= S.n || j >= S.n) ? 0.0 : (i == j ? -u[x] - 8.0 : -u[x]);
+    }
+}
+
+}  // namespace big
+}  // namespace mgpu

@@ -548,6 +548,7 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
 }  // namespace mgpu
 #include "kernels_frag.cuh"
 #include "kernels_cta.cuh"
+#include "kernels_big.cuh"
 namespace mgpu {
 
 __global__ void prep_reset_kernel(int *prep, int nsys)
@@ -587,9 +588,14 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int it
 // (NT, warps) of the one-CTA-per-matrix buckets, N = 8*NT up to 200
 #define MGPU_CTA_BUCKETS(X) X(6, 4) X(7, 4) X(8, 4) X(10, 8) X(12, 8) X(14, 8) X(16, 8) X(20, 16) X(25, 16)
 
+// NT of the large-N buckets (matrices in global memory, 64 pivots a round):
+// N up to 1024 in steps of 64
+#define MGPU_BIG_BUCKETS(X) X(32) X(40) X(48) X(56) X(64) X(72) X(80) X(88) X(96) X(104) X(112) X(120) X(128)
+
 // KIND_FRAG8: one warp per matrix; KIND_CTA8: one CTA per matrix (same 8x8
-// fragment data layout); KIND_TILE4: 4x4 register tiles.
-enum { KIND_TILE4 = 0, KIND_FRAG8 = 1, KIND_CTA8 = 2 };
+// fragment data layout); KIND_BIG: batched kernels over matrices held in
+// global memory (same layout); KIND_TILE4: 4x4 register tiles.
+enum { KIND_TILE4 = 0, KIND_FRAG8 = 1, KIND_CTA8 = 2, KIND_BIG = 3 };
 
 struct Bucket {
     int kind;
@@ -605,6 +611,9 @@ static const Bucket kBuckets[] = {
 #undef X
 #define X(nt, w) {KIND_CTA8, nt, w},
     MGPU_CTA_BUCKETS(X)
+#undef X
+#define X(nt) {KIND_BIG, nt, 0},
+    MGPU_BIG_BUCKETS(X)
 #undef X
 #define X(nt) {KIND_TILE4, nt, 0},
     MGPU_BUCKETS(X)
@@ -653,6 +662,7 @@ static cudaError_t set_smem(K kernel, size_t bytes)
 static cudaError_t launch_prep(int b, int max_nstep, int nsys, cudaStream_t st, const SysDev *sys, const int *list)
 {
     const int nt = kBuckets[b].nt;
+    if (kBuckets[b].kind == KIND_BIG) return cudaErrorInvalidValue;
     if (kBuckets[b].kind == KIND_CTA8) {
         dim3 grid(max_nstep, nsys);
         cudaError_t e = cudaSuccess;
@@ -698,6 +708,10 @@ static cudaError_t launch_prep(int b, int max_nstep, int nsys, cudaStream_t st, 
 // 4x4-tile kernels stage VL when it fits).
 static size_t prop_smem(int iprop, int b, int nham, int *vl_smem)
 {
+    if (kBuckets[b].kind == KIND_BIG) {
+        *vl_smem = 0;
+        return 0;
+    }
     if (kBuckets[b].kind == KIND_CTA8) {
         *vl_smem = 0;
         switch (kBuckets[b].nt) {
@@ -849,6 +863,23 @@ struct mgpu_plan {
     // per bucket ranges (jobs sorted by bucket, systems listed by bucket)
     std::vector<int> bucket_ids, job_begin, job_count, sys_begin, sys_count, max_nstep, vl_smem;
     std::vector<size_t> smem;
+    // large-N buckets (KIND_BIG): batched kernels over matrices in global memory
+    struct Big {
+        int slot = 0, b = 0, nt = 0, npad = 0, max_nstep = 0;
+        size_t td = 0;                       // doubles of one tiled matrix
+        int M = 0;                           // jobs
+        big::MatDesc *d_md = nullptr;        // per job: Y (MDPROP) or Z (LDPROP)
+        big::MatDesc *d_mduz = nullptr;      // LDPROP: [U of every job, Z of every job]
+        double *tiles = nullptr, *tiles2 = nullptr, *vec = nullptr;
+        int *ctr = nullptr;                  // [3][M]: pivot count, status, failing step
+        big::Panels pn{};
+        int pcap = 0;                        // matrices one round's scratch holds
+        std::vector<int> prep_sys;           // MDPROP: systems of this bucket ...
+        std::vector<big::MatDesc *> prep_md; // ... and the descriptors of their steps' U(C)
+    };
+    std::vector<Big> big;
+    int *d_kstep = nullptr;  // step counter read by the large-N kernels
+    int *d_kzero = nullptr;  // constant 0 (preparation batches)
     // host staging for run_host
     double *d_y = nullptr;
     int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
@@ -883,6 +914,25 @@ static cudaError_t upload(mgpu_plan *p, X **dst, const X *src, size_t count)
     return e;
 }
 
+// -A^{-1} in place for M matrices of a large-N bucket (64 pivots a round:
+// factor, panel and update kernels per round).
+static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::Panels &pn, const int *kstep,
+                              cudaStream_t st)
+{
+    const int rounds = nt / big::KB;
+    const int nbk = nt / 8;
+    for (int R = 0; R < rounds; ++R) {
+        big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn, R, kstep);
+        big::big_panel_kernel<<<dim3((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), 32 * big::PANEL_WARPS, 0,
+                                st>>>(md, pn, nt, R, kstep);
+        big::big_update_kernel<<<dim3(nbk * (nbk + 1) / 2, M), 32 * big::UPD_WARPS, big::kUpdSmem, st>>>(md, pn, nt,
+                                                                                                       R, kstep);
+    }
+    return cudaGetLastError();
+}
+
+static unsigned big_ew_blocks(size_t td) { return (unsigned)std::min<size_t>((td + big::EW_THREADS - 1) / big::EW_THREADS, 256); }
+
 static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g, int iprop)
 {
     if (!c || !g) return set_err(MGPU_ERR_ARG, "null system or grid");
@@ -895,8 +945,7 @@ static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g, int iprop)
     if (!g->rtab || (c->nham > 0 && !g->ptab)) return set_err(MGPU_ERR_ARG, "radial tables null");
     if (!(g->dr != 0.0) || !std::isfinite(g->dr)) return set_err(MGPU_ERR_ARG, "DR must be finite and non-zero");
     if (bucket_for(c->n, iprop) < 0)
-        return set_err(MGPU_ERR_UNSUPPORTED, iprop == MGPU_PROP_LDJ ? "N above 128 (largest LDPROP bucket)"
-                                                                     : "N above 200 (largest MDPROP bucket)");
+        return set_err(MGPU_ERR_UNSUPPORTED, "N above 1024 (largest compiled bucket)");
     return MGPU_OK;
 }
 
@@ -971,8 +1020,19 @@ int mgpu_plan_launches(const mgpu_plan *p)
     if (!p) return 0;
     int l = (p->iprop == MGPU_PROP_LDMD) ? 1 : 0;  // prep_reset_kernel
     for (size_t b = 0; b < p->bucket_ids.size(); ++b) {
+        if (kBuckets[p->bucket_ids[b]].kind == KIND_BIG) continue;
         if (p->iprop == MGPU_PROP_LDMD && p->sys_count[b] > 0) l += (p->sys_count[b] + 65534) / 65535;
         if (p->job_count[b] > 0) ++l;
+    }
+    for (const auto &g : p->big) {
+        const int per_inv = 3 * (g.nt / big::KB);
+        if (p->iprop == MGPU_PROP_LDMD)
+            for (size_t i = 0; i < g.prep_sys.size(); ++i) {
+                const int ns = p->sys_nstep[g.prep_sys[i]];
+                const int chunks = (ns + g.pcap - 1) / g.pcap;
+                l += chunks * (2 + per_inv);
+            }
+        if (g.M > 0) l += 3 + g.max_nstep * (4 + 2 * per_inv);
     }
     return l;
 }
@@ -1156,6 +1216,100 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         delete p;
         return set_err(MGPU_ERR_NOMEM, "uploading jobs", e);
     }
+    // large-N buckets: per-job tiled matrices and one round's scratch in device memory
+    constexpr int kPrepChunk = 128;  // U(C) steps inverted per preparation batch
+    for (size_t slot = 0; slot < p->bucket_ids.size(); ++slot) {
+        const int b = p->bucket_ids[slot];
+        if (kBuckets[b].kind != KIND_BIG) continue;
+        if (p->big.empty()) {
+            int zero[2] = {0, 0};
+            if ((e = upload(p, &p->d_kstep, zero, 1)) || (e = upload(p, &p->d_kzero, zero, 1)) ||
+                (e = set_smem(big::big_update_kernel, big::kUpdSmem)) ||
+                (e = set_smem(big::big_factor_kernel, big::kFactSmem))) {
+                delete p;
+                return set_err(MGPU_ERR_NOMEM, "large-N set-up", e);
+            }
+        }
+        mgpu_plan::Big g;
+        g.slot = (int)slot;
+        g.b = b;
+        g.nt = kBuckets[b].nt;
+        g.npad = bucket_npad(b);
+        g.td = matrix_elems(b);
+        g.M = p->job_count[slot];
+        g.max_nstep = p->max_nstep[slot];
+        const bool ldj = iprop == MGPU_PROP_LDJ;
+        if (g.M > 65535) {
+            delete p;
+            return set_err(MGPU_ERR_UNSUPPORTED, "more than 65535 large-N propagations in one plan bucket");
+        }
+        int maxsteps = 0;
+        for (int i = 0; i < p->sys_count[slot]; ++i) maxsteps = std::max(maxsteps, p->sys_nstep[syslist[p->sys_begin[slot] + i]]);
+        g.pcap = std::max((ldj ? 2 : 1) * g.M, ldj ? 1 : std::min(maxsteps, kPrepChunk));
+        const size_t fr = (size_t)g.nt * big::MC * 32;  // doubles of one operand panel
+        if ((e = p->dalloc(&g.pn.lam, (size_t)g.pcap * big::NB * big::NB)) ||
+            (e = p->dalloc(&g.pn.rd, (size_t)g.pcap * big::NB)) || (e = p->dalloc(&g.pn.xf, (size_t)g.pcap * fr)) ||
+            (e = p->dalloc(&g.pn.bf, (size_t)g.pcap * fr)) ||
+            (g.M && ((e = p->dalloc(&g.tiles, (size_t)g.M * g.td)) || (e = p->dalloc(&g.ctr, (size_t)3 * g.M)) ||
+                     (ldj && (e = p->dalloc(&g.tiles2, (size_t)g.M * g.td))) ||
+                     (!ldj && (e = p->dalloc(&g.vec, (size_t)g.M * 3 * g.npad)))))) {
+            delete p;
+            return set_err(MGPU_ERR_NOMEM, "allocating large-N matrices", e);
+        }
+        if (g.M) {
+            std::vector<big::MatDesc> md(g.M), uz;
+            for (int j = 0; j < g.M; ++j) {
+                const JobDev &jd = hj[p->job_begin[slot] + j];
+                big::MatDesc &d = md[j];
+                d.a = g.tiles + (size_t)j * g.td;
+                d.cnt = g.ctr + j;
+                d.stat = g.ctr + g.M + j;
+                d.kfail = g.ctr + 2 * g.M + j;
+                d.n = p->sys_n[jd.sys];
+                d.sign = 1;
+                d.nstep = p->sys_nstep[jd.sys];
+                d.kfix = 0;
+            }
+            if (ldj) {
+                uz = md;
+                for (int j = 0; j < g.M; ++j) {
+                    uz[j].a = g.tiles2 + (size_t)j * g.td;
+                    uz[j].sign = -1;
+                }
+                uz.insert(uz.end(), md.begin(), md.end());
+            }
+            if ((e = upload(p, &g.d_md, md.data(), md.size())) ||
+                (ldj && (e = upload(p, &g.d_mduz, uz.data(), uz.size())))) {
+                delete p;
+                return set_err(MGPU_ERR_NOMEM, "uploading large-N descriptors", e);
+            }
+        }
+        if (!ldj)
+            for (int i = 0; i < p->sys_count[slot]; ++i) {
+                const int sidx = syslist[p->sys_begin[slot] + i];
+                const int ns = p->sys_nstep[sidx];
+                std::vector<big::MatDesc> md(ns);
+                for (int k = 1; k <= ns; ++k) {
+                    big::MatDesc &d = md[k - 1];
+                    d.a = hs[sidx].q + (size_t)(k - 1) * g.td;
+                    d.cnt = p->d_prep + 3 * sidx;
+                    d.stat = p->d_prep + 3 * sidx + 1;
+                    d.kfail = p->d_prep + 3 * sidx + 2;
+                    d.n = p->sys_n[sidx];
+                    d.sign = 1;
+                    d.nstep = 0x7fffffff;
+                    d.kfix = k;
+                }
+                big::MatDesc *dm = nullptr;
+                if ((e = upload(p, &dm, md.data(), md.size()))) {
+                    delete p;
+                    return set_err(MGPU_ERR_NOMEM, "uploading preparation descriptors", e);
+                }
+                g.prep_sys.push_back(sidx);
+                g.prep_md.push_back(dm);
+            }
+        p->big.push_back(g);
+    }
     *out = p;
     return MGPU_OK;
 }
@@ -1179,7 +1333,7 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
         prep_reset_kernel<<<(p->nsys + 127) / 128, 128, 0, st>>>(p->d_prep, p->nsys);
         if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching prep_reset_kernel", e);
         for (size_t b = 0; b < p->bucket_ids.size(); ++b) {
-            if (p->sys_count[b] == 0) continue;
+            if (p->sys_count[b] == 0 || kBuckets[p->bucket_ids[b]].kind == KIND_BIG) continue;
             for (int s0 = 0; s0 < p->sys_count[b]; s0 += 65535) {
                 if ((e = launch_prep(p->bucket_ids[b], p->max_nstep[b], std::min(65535, p->sys_count[b] - s0), st,
                                      p->d_sys, p->d_syslists + p->sys_begin[b] + s0)))
@@ -1187,8 +1341,50 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
             }
         }
     }
+    if (p->iprop == MGPU_PROP_LDMD && (phases & 1))
+        for (const auto &g : p->big)
+            for (size_t i = 0; i < g.prep_sys.size(); ++i) {
+                const int s = g.prep_sys[i], ns = p->sys_nstep[s];
+                for (int k0 = 1; k0 <= ns; k0 += g.pcap) {
+                    const int c = std::min(g.pcap, ns - k0 + 1);
+                    const dim3 grid(big_ew_blocks(g.td), c);
+                    big::big_prep_build_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
+                    if ((e = big_invert(g.prep_md[i] + (k0 - 1), c, g.nt, g.pn, p->d_kzero, st)))
+                        return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
+                    big::big_prep_finish_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
+                    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
+                }
+            }
+    for (const auto &g : p->big) {
+        if (!(phases & 2) || g.M == 0) continue;
+        const bool ldj = p->iprop == MGPU_PROP_LDJ;
+        big::StepArgs a{p->d_sys, p->d_jobs + p->job_begin[g.slot], g.d_md, g.tiles2, g.vec, p->d_kstep, g.npad, g.td};
+        const dim3 ew(big_ew_blocks(g.td), g.M), ev((g.npad + big::EW_THREADS - 1) / big::EW_THREADS, g.M);
+        big::big_step_advance_kernel<<<1, 1, 0, st>>>(p->d_kstep, 1);
+        if (ldj) big::big_ldj_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y_dev);
+        else big::big_ldmd_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y_dev);
+        for (int k = 1; k <= g.max_nstep; ++k) {
+            if (ldj) {
+                big::big_ldj_pre_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+                if ((e = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, p->d_kstep, st))) break;  // U and Z
+                big::big_ldj_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                big::big_ldj_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+            } else {
+                big::big_ldmd_pre_kernel<<<ev, big::EW_THREADS, 0, st>>>(a);
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                big::big_ldmd_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                big::big_ldmd_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+            }
+            big::big_step_advance_kernel<<<1, 1, 0, st>>>(p->d_kstep, -1);
+        }
+        if (e || (e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
+        big::big_finish_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, ldj ? 1 : 0, y_dev, nodes_dev, status_dev, kfail_dev);
+        if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
+    }
     for (size_t b = 0; b < p->bucket_ids.size() && (phases & 2); ++b) {
-        if (p->job_count[b] == 0) continue;
+        if (p->job_count[b] == 0 || kBuckets[p->bucket_ids[b]].kind == KIND_BIG) continue;
         if ((e = launch_prop(p->iprop, p->bucket_ids[b], p->job_count[b], p->smem[b], p->vl_smem[b], st, p->d_sys,
                              p->d_jobs + p->job_begin[b], y_dev, nodes_dev, status_dev, kfail_dev)))
             return set_err(MGPU_ERR_CUDA, "launching the propagation kernel", e);
@@ -1379,7 +1575,9 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
         !ered_dev || !y_dev || !nodes_dev || !status_dev || !kfail_dev)
         return set_err(MGPU_ERR_ARG, "null device pointer");
     const int b = bucket_for(c->n);
-    if (b < 0) return set_err(MGPU_ERR_UNSUPPORTED, "N above the largest compiled bucket");
+    // the one-warp and one-CTA kernels only (N <= 200): the large-N kernels need per-job device matrices
+    if (b < 0 || kBuckets[b].kind == KIND_BIG)
+        return set_err(MGPU_ERR_UNSUPPORTED, "N above 200 (largest size of the allocation-free entry point)");
     const int nt = ntiles_of(b);
     const int npad = bucket_npad(b);
     const size_t tile = matrix_elems(b);  // doubles per tiled matrix

@@ -44,7 +44,7 @@ def test_library_is_sm100a_cuda(lib):
 
 def test_argument_validation_without_gpu(lib):
     from molscat_b200.propagators import Coupling, Segment, PropagatorError, Plan
-    assert lib.mgpu_max_n() >= 200
+    assert lib.mgpu_max_n() >= 1024
     n = lib.mgpu_max_n() + 1
     c = Coupling(n=n, nham=1, vl=np.zeros(n * (n + 1) // 2), eint=np.zeros(n), cent=np.zeros(n))
     seg = Segment(1, 0.1, np.array([1.0, 1.05, 1.1]), np.zeros((3, 1)))

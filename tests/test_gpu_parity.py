@@ -41,13 +41,13 @@ def oracle_prop(prop, c, seg, ered, y0):
 
 
 @pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
-@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 12, 17, 30, 31, 36, 40, 41, 45, 64, 80, 100, 128, 150, 200])
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 12, 17, 30, 31, 36, 40, 41, 45, 64, 80, 100, 128, 150, 200,
+                               201, 256, 300, 512])
 def test_random_systems(prop, n):
     """One warp per matrix (N <= 40), one CTA per matrix (N <= 200; LDPROP
-    <= 128), all on FP64 tensor cores."""
-    if prop == "LDJ" and n > 128:
-        pytest.skip("LDPROP keeps two matrices in shared memory: N <= 128")
-    nstep = 160 if n <= 64 else 60
+    <= 128), batched large-N kernels over matrices in global memory above
+    that; all on FP64 tensor cores."""
+    nstep = 160 if n <= 64 else (60 if n <= 300 else 20)
     c, seg, ered, y0 = cases.random_case(n, nstep, seed=1000 + n)
     yg, ng = propagate(prop, c, seg, ered, y0)
     yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
@@ -140,7 +140,7 @@ def test_rotor_full_grid(jtot, block, n):
 def test_batch_equals_alone():
     """Every job of a mixed batch (several N buckets, energies, both
     propagators' systems) gives exactly the result it gives alone."""
-    items = [cases.random_case(n, 120, seed=500 + n) for n in (3, 9, 16, 30, 33, 47, 90)]
+    items = [cases.random_case(n, 120, seed=500 + n) for n in (3, 9, 16, 30, 33, 47, 90, 260)]
     systems = [it[0] for it in items]
     segs = [it[1] for it in items]
     job_sys, job_e, y0s = [], [], []
@@ -184,8 +184,9 @@ def test_zero_pivot_reports_step_like_reference():
     assert st == 1 and kf == 1
 
 
-def test_nonfinite_potential_is_flagged():
-    c, seg, ered, y0 = cases.random_case(6, 50, seed=11)
+@pytest.mark.parametrize("n", [6, 260])
+def test_nonfinite_potential_is_flagged(n):
+    c, seg, ered, y0 = cases.random_case(n, 50, seed=11)
     ptab = seg.ptab.copy()
     ptab[41, 1] = np.nan
     bad = Segment(seg.nstep, seg.dr, seg.rtab, ptab)
@@ -197,9 +198,19 @@ def test_nonfinite_potential_is_flagged():
 
 
 def test_unsupported_size():
-    for prop, n in (("LDMD", _lib.load().mgpu_max_n() + 1), ("LDJ", 129)):
+    assert _lib.load().mgpu_max_n() == 1024
+    for prop, n in (("LDMD", 1025), ("LDJ", 1025)):
         c = Coupling(n=n, nham=1, vl=np.zeros(n * (n + 1) // 2), eint=np.zeros(n), cent=np.zeros(n))
         seg = Segment(1, 0.1, np.array([1.0, 1.05, 1.1]), np.zeros((3, 1)))
         with pytest.raises(PropagatorError) as e:
             propagate(prop, c, seg, 1.0, np.eye(n))
         assert e.value.status == _lib.MGPU_ERR_UNSUPPORTED
+
+
+def test_large_n_1024():
+    """The largest bucket (N = 1024, 16 rounds of 64 pivots per inversion)."""
+    c, seg, ered, y0 = cases.random_case(1024, 6, seed=1024)
+    yg, ng = propagate("LDMD", c, seg, ered, y0)
+    yo, no, st, _ = oracle_prop("LDMD", c, seg, ered, y0)
+    assert st == 0 and ng == no
+    assert cases.rel_err(yg, yo) < Y_TOL
