@@ -35,7 +35,7 @@ using wf::tix;
 constexpr int NB = 64;      // pivots per round
 constexpr int KB = NB / 8;  // tile columns per round
 constexpr int MC = NB / 4;  // m8n8k4 k-steps per round
-constexpr int FACT_THREADS = 256;
+constexpr int FACT_THREADS = 512;
 constexpr int PANEL_WARPS = 8;
 constexpr int UPD_WARPS = 4;
 constexpr int EW_THREADS = 256;
@@ -96,8 +96,28 @@ __device__ __forceinline__ void report_failure(const MatDesc &md, int flags, int
 
 // ---------------------------------------------------------------------------
 // factor: LDL^T of the 64x64 pivot block, Lam = L^{-1}, 1/delta
+// Sixteen sub-blocks of four pivots (the 4-pivot step of warp_dmma.cuh).  For
+// sub-block p: rows below form c = Lam4 D[i, p..p+3]; the trailing lower part
+// of D and the rows of Lam below take the rank-4 updates
+//     D_ij -= sum_m c_m(i) c_m(j)/delta_m ,  Lam_i -= sum_m (c_m(i)/delta_m) Lam_p+m
+// (elimination applied to I).  Look-ahead: warp 0 owns no trailing element;
+// while the other warps update, it updates the next 4x4 diagonal block first
+// and factors it (ldl_block4), so the chain of pivot reciprocals overlaps the
+// rank-4 updates.
 // ---------------------------------------------------------------------------
 constexpr size_t kFactSmem = 2 * (size_t)NB * (NB + 1) * sizeof(double);  // D and Lam, padded rows
+constexpr int kFactOwn = FACT_THREADS - 32;                                // threads owning elements
+constexpr int kFactD = (NB * (NB + 1) / 2 + kFactOwn - 1) / kFactOwn;      // D elements per thread
+constexpr int kFactL = (NB * (NB - 1) / 2 + kFactOwn - 1) / kFactOwn;      // Lam elements per thread
+
+__device__ __forceinline__ void tri_rc(int e, int &i, int &j)  // e -> (i, j), j <= i
+{
+    int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+    while (r * (r + 1) / 2 > e) --r;
+    while ((r + 1) * (r + 2) / 2 <= e) ++r;
+    i = r;
+    j = e - r * (r + 1) / 2;
+}
 
 __global__ void __launch_bounds__(FACT_THREADS)
 big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const int *__restrict__ kstep)
@@ -105,41 +125,148 @@ big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const i
     extern __shared__ __align__(16) double fsm[];
     double (*D)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm);
     double (*L)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm + NB * (NB + 1));
+    __shared__ __align__(16) double s_c[NB][4];  // c(i) of the current sub-block
+    __shared__ __align__(16) double s_t[NB][4];  // c(i) / delta
+    __shared__ double s_f[16];                   // ldl_block4 operands of the current sub-block
+    __shared__ double s_r[NB];
     __shared__ int s_cnt, s_flags;
     const MatDesc md = mds[blockIdx.x];
     const int k = *kstep;
     if (k > md.nstep) return;
     const int p0 = NB * round, K0 = KB * round;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) s_cnt = s_flags = 0;
     for (int x = tid; x < NB * NB; x += FACT_THREADS) {
         const int i = x >> 6, j = x & 63;
         double v = 0.0;
         if (j <= i) v = md.a[(size_t)tix(K0 + (i >> 3), K0 + (j >> 3)) * 64 + ((i & 7) * 4 + ((j & 7) >> 1)) * 2 + (j & 1)];
-        if (i == j && p0 + i >= md.n) v = 1.0;  // padding pivot
         D[i][j] = v;
         L[i][j] = (i == j) ? 1.0 : 0.0;
     }
-    if (tid == 0) s_cnt = s_flags = 0;
-    // thread -> row i, columns j = c0 (mod 4)
-    const int i = tid >> 2, c0 = tid & 3;
-    for (int kk = 0; kk < NB; ++kk) {
-        __syncthreads();
-        const double dk = D[kk][kk];
-        const double rk = pivot_reciprocal(dk);
-        if (tid == 0) {
-            if (p0 + kk < md.n && dk < 0.0) ++s_cnt;
-            s_flags |= pivot_flags(dk);
+    // owned elements (packed (i << 8) | j, -1 when none): D lower triangle, Lam strictly lower
+    int od[kFactD], ol[kFactL];
+#pragma unroll
+    for (int u = 0; u < kFactD; ++u) {
+        const int e = (tid - 32) + u * kFactOwn;
+        int i = 0, j = 0;
+        const bool ok = warp > 0 && e < NB * (NB + 1) / 2;
+        if (ok) tri_rc(e, i, j);
+        od[u] = ok ? ((i << 8) | j) : -1;
+    }
+#pragma unroll
+    for (int u = 0; u < kFactL; ++u) {
+        const int e = (tid - 32) + u * kFactOwn;
+        int i = 0, c = 0;
+        const bool ok = warp > 0 && e < NB * (NB - 1) / 2;
+        if (ok) tri_rc(e, i, c);
+        ol[u] = ok ? (((i + 1) << 8) | c) : -1;
+    }
+    __syncthreads();
+    // warp 0 factors one 4x4 diagonal sub-block (rows q..q+3 of D final)
+    auto sub_factor = [&](int q) {
+        double f[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j <= i; ++j) f[i][j] = D[q + i][q + j];
+        int cnt = 0, flags = 0;
+        wf::ldl_block4(f, md.n - p0 - q, cnt, flags);
+        if (lane == 0) {
+            s_cnt += cnt;
+            s_flags |= flags;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) s_f[i * 4 + j] = f[i][j];
         }
-        if (i > kk) {
-            const double li = D[i][kk] * rk;
-            for (int j = kk + 1 + ((c0 - kk - 1) & 3); j <= i; j += 4) D[i][j] = fma(-li, D[j][kk], D[i][j]);
-            for (int c = c0; c <= kk; c += 4) L[i][c] = fma(-li, L[kk][c], L[i][c]);
+    };
+    if (warp == 0) sub_factor(0);
+    for (int sb = 0; sb < NB / 4; ++sb) {
+        const int p = 4 * sb;
+        __syncthreads();
+        double f[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) f[i][j] = s_f[i * 4 + j];
+        if (tid < 4) s_r[p + tid] = (tid == 0) ? f[0][0] : (tid == 1) ? f[1][1] : (tid == 2) ? f[2][2] : f[3][3];
+        // c(i) = Lam4 D[i, p..p+3] for rows below; Lam rows of the sub-block = Lam4 Lam_sub
+        if (tid < 4 * NB) {
+            const int i = tid >> 2, m = tid & 3;
+            if (i >= p + 4) {
+                double lq[3], rq;
+                wf::lane_operands(f, m, lq, rq);  // row m of Lam4 below the diagonal, 1/delta_m
+                const double c = fma(lq[0], D[i][p], fma(lq[1], D[i][p + 1], fma(lq[2], D[i][p + 2], D[i][p + m])));
+                s_c[i][m] = c;
+                s_t[i][m] = c * rq;
+            }
+        } else {
+            // one column per thread, in place from the last row up (row m reads the old rows above it)
+            const int c = tid - 4 * NB;
+            if (c < p + 4) {
+#pragma unroll
+                for (int m = 3; m >= 1; --m) {
+                    double v = L[p + m][c];
+#pragma unroll
+                    for (int mm = 0; mm < 3; ++mm)
+                        if (mm < m) v = fma(f[m][mm], L[p + mm][c], v);
+                    L[p + m][c] = v;
+                }
+            }
+        }
+        __syncthreads();
+        const int q = p + 4;  // next sub-block
+        if (warp == 0) {
+            if (q < NB) {
+                if (lane < 10) {
+                    int ii, jj;
+                    tri_rc(lane, ii, jj);
+                    const int i = q + ii, j = q + jj;
+                    double v = D[i][j];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) v = fma(-s_t[i][m], s_c[j][m], v);
+                    D[i][j] = v;
+                }
+                __syncwarp();
+                sub_factor(q);
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < kFactD; ++u) {
+                const int i = od[u] >> 8, j = od[u] & 255;
+                if (od[u] >= 0 && j >= q && !(i < q + 4)) {  // the next diagonal block is warp 0's
+                    const double2 t01 = *reinterpret_cast<const double2 *>(&s_t[i][0]);
+                    const double2 t23 = *reinterpret_cast<const double2 *>(&s_t[i][2]);
+                    const double2 c01 = *reinterpret_cast<const double2 *>(&s_c[j][0]);
+                    const double2 c23 = *reinterpret_cast<const double2 *>(&s_c[j][2]);
+                    double v = D[i][j];
+                    v = fma(-t01.x, c01.x, v);
+                    v = fma(-t01.y, c01.y, v);
+                    v = fma(-t23.x, c23.x, v);
+                    v = fma(-t23.y, c23.y, v);
+                    D[i][j] = v;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFactL; ++u) {
+                const int i = ol[u] >> 8, c = ol[u] & 255;
+                if (ol[u] >= 0 && i >= q && c < q) {
+                    const double2 t01 = *reinterpret_cast<const double2 *>(&s_t[i][0]);
+                    const double2 t23 = *reinterpret_cast<const double2 *>(&s_t[i][2]);
+                    double v = L[i][c];
+                    v = fma(-t01.x, L[p][c], v);
+                    v = fma(-t01.y, L[p + 1][c], v);
+                    v = fma(-t23.x, L[p + 2][c], v);
+                    v = fma(-t23.y, L[p + 3][c], v);
+                    L[i][c] = v;
+                }
+            }
         }
     }
     __syncthreads();
     double *lam = pn.lam + (size_t)blockIdx.x * NB * NB;
     for (int x = tid; x < NB * NB; x += FACT_THREADS) lam[x] = L[x >> 6][x & 63];
-    if (tid < NB) pn.rd[(size_t)blockIdx.x * NB + tid] = pivot_reciprocal(D[tid][tid]);
+    if (tid < NB) pn.rd[(size_t)blockIdx.x * NB + tid] = s_r[tid];
     if (tid == 0) {
         if (s_cnt) atomicAdd(md.cnt, md.sign * s_cnt);
         if (s_flags) report_failure(md, s_flags, k);
@@ -186,12 +313,15 @@ big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, 
 #pragma unroll
     for (int kt = 0; kt < KB; ++kt) acc[kt][0] = acc[kt][1] = 0.0;
     const int i = 8 * I + r;
-#pragma unroll 4
-    for (int mc = 0; mc < MC; ++mc) {
-        const double v = md.a[sym_index(i, p0 + 4 * mc + q)];  // A[i, p0 + 4mc + q] (A fragment)
+    double v[MC];  // A[i, p0 + 4mc + q] (A fragments), all loads in flight together
 #pragma unroll
-        for (int kt = 0; kt < KB; ++kt) wf::dmma(acc[kt][0], acc[kt][1], v, lamB[kt][mc][lane]);
-    }
+    for (int mc = 0; mc < MC; ++mc) v[mc] = md.a[sym_index(i, p0 + 4 * mc + q)];
+    // Lam is unit lower triangular: output columns 8kt..8kt+7 need k-steps mc <= 2kt+1 only
+#pragma unroll
+    for (int mc = 0; mc < MC; ++mc)
+#pragma unroll
+        for (int kt = 0; kt < KB; ++kt)
+            if (mc <= 2 * kt + 1) wf::dmma(acc[kt][0], acc[kt][1], v[mc], lamB[kt][mc][lane]);
     // acc[kt][s] = c(8I + r, 8kt + 2q + s) -> A-fragment slot (k-step 2kt + q/2, lane r*4 + 2(q&1) + s)
 #pragma unroll
     for (int kt = 0; kt < KB; ++kt) {
@@ -208,8 +338,13 @@ big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, 
 constexpr uint32_t kUpdHalfBytes = KB * MC * 32 * sizeof(double);  // 32 KB: 8 tile rows of X (or B)
 constexpr size_t kUpdSmem = 2 * (size_t)kUpdHalfBytes;
 
+// Which 64x64 blocks of tiles a launch updates: all of them, only block row and
+// column `cblk` (grid.x = NT/8), or all but those (the look-ahead split).
+enum { UPD_ALL = 0, UPD_ONLY = 1, UPD_EXCEPT = 2 };
+
 __global__ void __launch_bounds__(32 * UPD_WARPS)
-big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep)
+big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep,
+                  int mode, int cblk)
 {
     extern __shared__ __align__(128) double usm[];
     __shared__ __align__(8) uint64_t bar;
@@ -217,7 +352,14 @@ big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round,
     const MatDesc md = mds[m];
     if (*kstep > md.nstep) return;
     int BI, BJ;
-    tile_ij(blockIdx.x, BI, BJ);
+    if (mode == UPD_ONLY) {
+        const int x = blockIdx.x;
+        BI = x <= cblk ? cblk : x;
+        BJ = x <= cblk ? x : cblk;
+    } else {
+        tile_ij(blockIdx.x, BI, BJ);
+        if (mode == UPD_EXCEPT && (BI == cblk || BJ == cblk)) return;  // whole CTA
+    }
     double *Xs = usm, *Bs = usm + KB * MC * 32;
     if (threadIdx.x == 0) {
         mbar_init(&bar, 2);

@@ -872,12 +872,14 @@ struct mgpu_plan {
         big::MatDesc *d_mduz = nullptr;      // LDPROP: [U of every job, Z of every job]
         double *tiles = nullptr, *tiles2 = nullptr, *vec = nullptr;
         int *ctr = nullptr;                  // [3][M]: pivot count, status, failing step
-        big::Panels pn{};
+        big::Panels pn[2]{};                 // shared Lam / 1/delta, X and B twice (look-ahead)
         int pcap = 0;                        // matrices one round's scratch holds
         std::vector<int> prep_sys;           // MDPROP: systems of this bucket ...
         std::vector<big::MatDesc *> prep_md; // ... and the descriptors of their steps' U(C)
     };
     std::vector<Big> big;
+    cudaStream_t side = nullptr;           // look-ahead stream of the large-N inversions
+    cudaEvent_t evf = nullptr, evj = nullptr;
     int *d_kstep = nullptr;  // step counter read by the large-N kernels
     int *d_kzero = nullptr;  // constant 0 (preparation batches)
     // host staging for run_host
@@ -888,6 +890,9 @@ struct mgpu_plan {
 
     ~mgpu_plan()
     {
+        if (evf) cudaEventDestroy(evf);
+        if (evj) cudaEventDestroy(evj);
+        if (side) cudaStreamDestroy(side);
         for (void *p : allocs) cudaFree(p);
         if (d_y) cudaFree(d_y);
         if (d_nodes) cudaFree(d_nodes);
@@ -914,19 +919,34 @@ static cudaError_t upload(mgpu_plan *p, X **dst, const X *src, size_t count)
     return e;
 }
 
-// -A^{-1} in place for M matrices of a large-N bucket (64 pivots a round:
-// factor, panel and update kernels per round).
-static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::Panels &pn, const int *kstep,
-                              cudaStream_t st)
+// -A^{-1} in place for M matrices of a large-N bucket, 64 pivots a round
+// (factor, panel and update kernels).  Look-ahead: once the tile row and
+// column that form the next round's panel are updated, the next round's
+// factor and panel run on the high-priority `side` stream while `st` updates
+// the remaining tiles; the X/B operands alternate between two buffers.
+static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::Panels (&pn)[2], const int *kstep,
+                              cudaStream_t st, cudaStream_t side, cudaEvent_t evf, cudaEvent_t evj)
 {
     const int rounds = nt / big::KB;
     const int nbk = nt / 8;
+    const dim3 gp((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), gall(nbk * (nbk + 1) / 2, M), gcol(nbk, M);
+    const int ut = 32 * big::UPD_WARPS, pt = 32 * big::PANEL_WARPS;
+    cudaError_t e;
+    big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn[0], 0, kstep);
+    big::big_panel_kernel<<<gp, pt, 0, st>>>(md, pn[0], nt, 0, kstep);
     for (int R = 0; R < rounds; ++R) {
-        big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn, R, kstep);
-        big::big_panel_kernel<<<dim3((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), 32 * big::PANEL_WARPS, 0,
-                                st>>>(md, pn, nt, R, kstep);
-        big::big_update_kernel<<<dim3(nbk * (nbk + 1) / 2, M), 32 * big::UPD_WARPS, big::kUpdSmem, st>>>(md, pn, nt,
-                                                                                                       R, kstep);
+        const big::Panels &cur = pn[R & 1], &nxt = pn[(R + 1) & 1];
+        if (R + 1 < rounds) {
+            big::big_update_kernel<<<gcol, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_ONLY, R + 1);
+            if ((e = cudaEventRecord(evf, st)) || (e = cudaStreamWaitEvent(side, evf, 0))) return e;
+            big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, side>>>(md, nxt, R + 1, kstep);
+            big::big_panel_kernel<<<gp, pt, 0, side>>>(md, nxt, nt, R + 1, kstep);
+            if ((e = cudaEventRecord(evj, side))) return e;
+            big::big_update_kernel<<<gall, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_EXCEPT, R + 1);
+            if ((e = cudaStreamWaitEvent(st, evj, 0))) return e;
+        } else {
+            big::big_update_kernel<<<gall, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_ALL, -1);
+        }
     }
     return cudaGetLastError();
 }
@@ -1025,7 +1045,7 @@ int mgpu_plan_launches(const mgpu_plan *p)
         if (p->job_count[b] > 0) ++l;
     }
     for (const auto &g : p->big) {
-        const int per_inv = 3 * (g.nt / big::KB);
+        const int per_inv = 4 * (g.nt / big::KB) - 1;  // factor, panel, two update launches; one update in the last round
         if (p->iprop == MGPU_PROP_LDMD)
             for (size_t i = 0; i < g.prep_sys.size(); ++i) {
                 const int ns = p->sys_nstep[g.prep_sys[i]];
@@ -1222,8 +1242,12 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         const int b = p->bucket_ids[slot];
         if (kBuckets[b].kind != KIND_BIG) continue;
         if (p->big.empty()) {
-            int zero[2] = {0, 0};
-            if ((e = upload(p, &p->d_kstep, zero, 1)) || (e = upload(p, &p->d_kzero, zero, 1)) ||
+            int zero[2] = {0, 0}, lo = 0, hi = 0;
+            if ((e = cudaDeviceGetStreamPriorityRange(&lo, &hi)) ||
+                (e = cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, hi)) ||
+                (e = cudaEventCreateWithFlags(&p->evf, cudaEventDisableTiming)) ||
+                (e = cudaEventCreateWithFlags(&p->evj, cudaEventDisableTiming)) ||
+                (e = upload(p, &p->d_kstep, zero, 1)) || (e = upload(p, &p->d_kzero, zero, 1)) ||
                 (e = set_smem(big::big_update_kernel, big::kUpdSmem)) ||
                 (e = set_smem(big::big_factor_kernel, big::kFactSmem))) {
                 delete p;
@@ -1247,15 +1271,18 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         for (int i = 0; i < p->sys_count[slot]; ++i) maxsteps = std::max(maxsteps, p->sys_nstep[syslist[p->sys_begin[slot] + i]]);
         g.pcap = std::max((ldj ? 2 : 1) * g.M, ldj ? 1 : std::min(maxsteps, kPrepChunk));
         const size_t fr = (size_t)g.nt * big::MC * 32;  // doubles of one operand panel
-        if ((e = p->dalloc(&g.pn.lam, (size_t)g.pcap * big::NB * big::NB)) ||
-            (e = p->dalloc(&g.pn.rd, (size_t)g.pcap * big::NB)) || (e = p->dalloc(&g.pn.xf, (size_t)g.pcap * fr)) ||
-            (e = p->dalloc(&g.pn.bf, (size_t)g.pcap * fr)) ||
+        if ((e = p->dalloc(&g.pn[0].lam, (size_t)g.pcap * big::NB * big::NB)) ||
+            (e = p->dalloc(&g.pn[0].rd, (size_t)g.pcap * big::NB)) || (e = p->dalloc(&g.pn[0].xf, (size_t)g.pcap * fr)) ||
+            (e = p->dalloc(&g.pn[0].bf, (size_t)g.pcap * fr)) || (e = p->dalloc(&g.pn[1].xf, (size_t)g.pcap * fr)) ||
+            (e = p->dalloc(&g.pn[1].bf, (size_t)g.pcap * fr)) ||
             (g.M && ((e = p->dalloc(&g.tiles, (size_t)g.M * g.td)) || (e = p->dalloc(&g.ctr, (size_t)3 * g.M)) ||
                      (ldj && (e = p->dalloc(&g.tiles2, (size_t)g.M * g.td))) ||
                      (!ldj && (e = p->dalloc(&g.vec, (size_t)g.M * 3 * g.npad)))))) {
             delete p;
             return set_err(MGPU_ERR_NOMEM, "allocating large-N matrices", e);
         }
+        g.pn[1].lam = g.pn[0].lam;
+        g.pn[1].rd = g.pn[0].rd;
         if (g.M) {
             std::vector<big::MatDesc> md(g.M), uz;
             for (int j = 0; j < g.M; ++j) {
@@ -1349,7 +1376,7 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
                     const int c = std::min(g.pcap, ns - k0 + 1);
                     const dim3 grid(big_ew_blocks(g.td), c);
                     big::big_prep_build_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
-                    if ((e = big_invert(g.prep_md[i] + (k0 - 1), c, g.nt, g.pn, p->d_kzero, st)))
+                    if ((e = big_invert(g.prep_md[i] + (k0 - 1), c, g.nt, g.pn, p->d_kzero, st, p->side, p->evf, p->evj)))
                         return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
                     big::big_prep_finish_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
                     if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
@@ -1366,15 +1393,15 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
         for (int k = 1; k <= g.max_nstep; ++k) {
             if (ldj) {
                 big::big_ldj_pre_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, p->d_kstep, st))) break;  // U and Z
+                if ((e = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;  // U and Z
                 big::big_ldj_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
                 big::big_ldj_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
             } else {
                 big::big_ldmd_pre_kernel<<<ev, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
                 big::big_ldmd_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st))) break;
+                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
                 big::big_ldmd_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
             }
             big::big_step_advance_kernel<<<1, 1, 0, st>>>(p->d_kstep, -1);
