@@ -169,6 +169,51 @@ int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, int njobs,
                         const double *ered_dev, double *y_dev, int *nodes_dev,
                         int *status_dev, int *kfail_dev, void *stream);
 
+/* ---- request server (continuous batching) --------------------------------
+ * No counterpart in the reference: its drivers call MDPROP/LDPROP once per
+ * (JTOT, parity block, energy) in sequence (mol.driver.f:1181-1855,
+ * scctrl.f:173,185).  The server keeps registered systems on the device
+ * (VL/IV tiles, EINT/CENT, radial tables and, for MDPROP, the energy-
+ * independent 2HQ(C) table, computed once per system) and runs single
+ * propagations submitted at any time.  A scheduler thread forms batches of
+ * pending requests of one N-bucket (oldest request first), launches each
+ * batch on its own stream as soon as a stream slot and enough of the HBM
+ * budget are free, and retires batches as they finish, so requests that
+ * arrive while others run are admitted without waiting for them and their
+ * work overlaps on the device.  A request's result does not depend on the
+ * batch it runs in.
+ *
+ * mgpu_server_create: iprop MGPU_PROP_LDMD or MGPU_PROP_LDJ; hbm_budget_bytes caps
+ *   the device memory of batches in flight (registered systems come on top);
+ *   `streams` concurrent batches, at most max_batch requests each, at most
+ *   max_systems registered systems.
+ * mgpu_server_add_system: uploads one system (same arguments as mgpu_mdprop)
+ *   and returns its id; blocks until its preparation is done.
+ * mgpu_submit: queues one propagation; Y0 (N*N, column-major, host) is
+ *   copied, the host outputs y_out (N*N), nodes, status, kfail must stay
+ *   valid until the request completes.  *ticket identifies the request.
+ * mgpu_poll: 1 when the request is complete, 0 while queued or running.
+ * mgpu_wait: blocks until complete; returns MGPU_OK or the error that kept the
+ *   request from running (MGPU_ERR_NOMEM when it alone exceeds the budget);
+ *   the propagation's own status (zero pivot, ...) is in *status.
+ * mgpu_request_times: t3 = {submitted, launched, completed}, seconds on the
+ *   host's steady clock.
+ * mgpu_release: forgets a completed request.
+ * mgpu_server_in_flight: batches on the device, queued requests, bytes in use.
+ * mgpu_server_destroy: waits for the work in flight, frees everything. */
+typedef struct mgpu_server mgpu_server;
+int mgpu_server_create(mgpu_server **server, int iprop, size_t hbm_budget_bytes, int streams, int max_batch,
+                       int max_systems);
+void mgpu_server_destroy(mgpu_server *server);
+int mgpu_server_add_system(mgpu_server *server, const mgpu_coupling *c, const mgpu_grid *g, int *sys_id);
+int mgpu_submit(mgpu_server *server, int sys_id, double ered, const double *y0, double *y_out, int *nodes,
+                int *status, int *kfail, long long *ticket);
+int mgpu_poll(mgpu_server *server, long long ticket);
+int mgpu_wait(mgpu_server *server, long long ticket);
+int mgpu_request_times(mgpu_server *server, long long ticket, double *t3);
+int mgpu_release(mgpu_server *server, long long ticket);
+int mgpu_server_in_flight(mgpu_server *server, int *batches, int *queued, size_t *bytes);
+
 /* Kernel family for the sizes two families cover (N <= 64): 0 = FP64
  * tensor-core (DMMA) 8x8 fragments, one warp (N <= 40) or one CTA per
  * matrix (the default); 1 = 4x4 register tiles with the scalar sweep.

@@ -45,6 +45,8 @@ EXPORTS = (
     "mgpu_plan_flops", "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
     "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
     "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc", "mgpu_set_kernel_family",
+    "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
+    "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight",
 )
 
 _lib = None
@@ -88,6 +90,18 @@ def load(path: str | None = None):
     L.mgpu_last_error.restype = ctypes.c_char_p
     L.mgpu_max_n.argtypes = []
     L.mgpu_set_kernel_family.argtypes = [ctypes.c_int]
+    ll = ctypes.c_longlong
+    L.mgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int]
+    L.mgpu_server_destroy.argtypes = [vp]
+    L.mgpu_server_destroy.restype = None
+    L.mgpu_server_add_system.argtypes = [vp, pc, pg, _ip]
+    L.mgpu_submit.argtypes = [vp, ctypes.c_int, ctypes.c_double, _dp, _dp, _ip, _ip, _ip, ctypes.POINTER(ll)]
+    L.mgpu_poll.argtypes = [vp, ll]
+    L.mgpu_wait.argtypes = [vp, ll]
+    L.mgpu_request_times.argtypes = [vp, ll, _dp]
+    L.mgpu_release.argtypes = [vp, ll]
+    L.mgpu_server_in_flight.argtypes = [vp, _ip, _ip, ctypes.POINTER(ctypes.c_size_t)]
     if path is None:
         _lib = L
     return L

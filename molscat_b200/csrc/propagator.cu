@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <new>
 #include <string>
@@ -648,14 +649,28 @@ static int bucket_for(int n, int iprop = MGPU_PROP_LDMD)
     return -1;
 }
 
+// Raise a kernel's dynamic shared-memory limit, once per (device, kernel)
+// and size: setting attributes again on every launch is not free, and a
+// launch path that runs beside other work should not touch a kernel that is
+// executing.
 template <class K>
 static cudaError_t set_smem(K kernel, size_t bytes)
 {
     if (bytes <= 48 * 1024) return cudaSuccess;
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<int, const void *>, size_t>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const void *key = (const void *)kernel;
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto &d : done)
+        if (d.first.first == dev && d.first.second == key && d.second >= bytes) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     // resident CTAs are limited by registers, not by the L1/shared split
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+    if (e == cudaSuccess) done.push_back({{dev, key}, bytes});
+    return e;
 }
 
 // grid.x counts steps, grid.y systems
@@ -845,6 +860,47 @@ static int set_err(int code, const char *what, cudaError_t e = cudaSuccess)
     return code;
 }
 
+// Device state of one large-N bucket of a run: per-job tiled matrices, one
+// round's scratch (X/B twice for the look-ahead), descriptors, step counter.
+struct BigBucket {
+    int b = 0, nt = 0, npad = 0, max_nstep = 0;
+    size_t td = 0;                        // doubles of one tiled matrix
+    int M = 0;                            // jobs
+    const JobDev *d_jobs = nullptr;       // this bucket's jobs
+    big::MatDesc *d_md = nullptr;         // per job: Y (MDPROP) or Z (LDPROP)
+    big::MatDesc *d_mduz = nullptr;       // LDPROP: [U of every job, Z of every job]
+    double *tiles = nullptr, *tiles2 = nullptr, *vec = nullptr;
+    int *ctr = nullptr;                   // [3][M]: pivot count, status, failing step
+    big::Panels pn[2]{};                  // shared Lam / 1/delta, X and B twice
+    int pcap = 0;                         // matrices one round's scratch holds
+    int *kstep = nullptr, *kzero = nullptr;
+    cudaGraphExec_t step_graph = nullptr; // one step of the loop, captured once, replayed NSTEP times
+    std::vector<int> prep_sys;            // MDPROP: systems whose U(C) this bucket prepares ...
+    std::vector<big::MatDesc *> prep_md;  // ... and the descriptors of their steps
+};
+
+// Device allocation and host -> device upload, injected so that plans
+// (synchronous) and server batches (stream-ordered) share the set-up code.
+using AllocFn = std::function<cudaError_t(void **, size_t)>;
+using UploadFn = std::function<cudaError_t(void *, const void *, size_t)>;
+
+template <class X>
+static cudaError_t alloc_n(const AllocFn &al, X **p, size_t n)
+{
+    void *q = nullptr;
+    cudaError_t e = al(&q, std::max<size_t>(n, 1) * sizeof(X));
+    *p = (X *)q;
+    return e;
+}
+
+template <class X>
+static cudaError_t put_n(const AllocFn &al, const UploadFn &up, X **p, const X *src, size_t n)
+{
+    cudaError_t e = alloc_n(al, p, n);
+    if (e == cudaSuccess && n) e = up(*p, src, n * sizeof(X));
+    return e;
+}
+
 struct mgpu_plan {
     int iprop = 0;
     int nsys = 0, njobs = 0;
@@ -863,25 +919,10 @@ struct mgpu_plan {
     // per bucket ranges (jobs sorted by bucket, systems listed by bucket)
     std::vector<int> bucket_ids, job_begin, job_count, sys_begin, sys_count, max_nstep, vl_smem;
     std::vector<size_t> smem;
-    // large-N buckets (KIND_BIG): batched kernels over matrices in global memory
-    struct Big {
-        int slot = 0, b = 0, nt = 0, npad = 0, max_nstep = 0;
-        size_t td = 0;                       // doubles of one tiled matrix
-        int M = 0;                           // jobs
-        big::MatDesc *d_md = nullptr;        // per job: Y (MDPROP) or Z (LDPROP)
-        big::MatDesc *d_mduz = nullptr;      // LDPROP: [U of every job, Z of every job]
-        double *tiles = nullptr, *tiles2 = nullptr, *vec = nullptr;
-        int *ctr = nullptr;                  // [3][M]: pivot count, status, failing step
-        big::Panels pn[2]{};                 // shared Lam / 1/delta, X and B twice (look-ahead)
-        int pcap = 0;                        // matrices one round's scratch holds
-        std::vector<int> prep_sys;           // MDPROP: systems of this bucket ...
-        std::vector<big::MatDesc *> prep_md; // ... and the descriptors of their steps' U(C)
-    };
-    std::vector<Big> big;
+    std::vector<BigBucket> big;            // large-N buckets (KIND_BIG)
     cudaStream_t side = nullptr;           // look-ahead stream of the large-N inversions
-    cudaEvent_t evf = nullptr, evj = nullptr;
-    int *d_kstep = nullptr;  // step counter read by the large-N kernels
-    int *d_kzero = nullptr;  // constant 0 (preparation batches)
+    cudaStream_t own = nullptr;            // the large-N work (never the legacy stream: graph capture)
+    cudaEvent_t evf = nullptr, evj = nullptr, ev_in = nullptr, ev_out = nullptr;
     // host staging for run_host
     double *d_y = nullptr;
     int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
@@ -890,9 +931,15 @@ struct mgpu_plan {
 
     ~mgpu_plan()
     {
+        if (own) cudaStreamSynchronize(own);
+        for (auto &g : big)
+            if (g.step_graph) cudaGraphExecDestroy(g.step_graph);
         if (evf) cudaEventDestroy(evf);
         if (evj) cudaEventDestroy(evj);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
         if (side) cudaStreamDestroy(side);
+        if (own) cudaStreamDestroy(own);
         for (void *p : allocs) cudaFree(p);
         if (d_y) cudaFree(d_y);
         if (d_nodes) cudaFree(d_nodes);
@@ -952,6 +999,243 @@ static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::
 }
 
 static unsigned big_ew_blocks(size_t td) { return (unsigned)std::min<size_t>((td + big::EW_THREADS - 1) / big::EW_THREADS, 256); }
+
+// One system in bucket b's tile layout on the device: VL/IV tiled (sumlam.f
+// pair order), EINT/CENT padded, radial tables, MDPROP 2HQ(C) storage.
+static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, int b, SysDev &d, const AllocFn &al,
+                        const UploadFn &up)
+{
+    const int npad = bucket_npad(b);
+    const int nt = ntiles_of(b);
+    const size_t TT = tile_elems(b);
+    const size_t tsz = (size_t)std::max(c.nham, 1) * TT * nt;
+    std::vector<double> vlt(tsz, 0.0);
+    std::vector<int> ivt(c.ivlfl > 0 ? tsz : 1, 0);
+    for (int t = 0; t < nt; ++t)
+        for (int ee = 0; ee < (int)TT; ++ee) {
+            int i = 0, j = 0;
+            tile_element(b, t, ee, &i, &j);
+            if (i >= c.n || j >= c.n) continue;
+            const int lo = std::min(i, j), hi = std::max(i, j);
+            // pair (row lo, column hi) of the packed upper triangle (sumlam.f:33-36,74-86)
+            const size_t pair = (size_t)hi * (hi + 1) / 2 + lo;
+            for (int l = 0; l < c.nham; ++l) {
+                const size_t src = pair * c.nvlblk + l;
+                const size_t dst = tile_offset(b, l, t, ee);
+                vlt[dst] = c.vl[src];
+                if (c.ivlfl > 0) {
+                    const int ix = c.iv[src] - 1;
+                    if (ix < 0 || ix >= c.nham) return set_err(MGPU_ERR_ARG, "IV index outside 1..NHAM");
+                    ivt[dst] = ix;
+                }
+            }
+        }
+    std::vector<double> eint(npad, 0.0), cent(npad, 0.0);
+    std::copy(c.eint, c.eint + c.n, eint.begin());
+    std::copy(c.cent, c.cent + c.n, cent.begin());
+    memset(&d, 0, sizeof d);
+    d.n = c.n;
+    d.nham = c.nham;
+    d.ivlfl = c.ivlfl;
+    d.nconst = c.nconst;
+    d.nrsq = c.nrsq;
+    d.nstep = g.nstep;
+    d.ntiles = nt;
+    d.kind = frag_layout(b) ? 1 : 0;
+    d.conlen = c.conlen;
+    d.dr = g.dr;
+    const size_t nr = 2 * (size_t)g.nstep + 1;
+    double *dv = nullptr, *de = nullptr, *dc = nullptr, *drt = nullptr, *dpt = nullptr, *dq = nullptr;
+    int *di = nullptr;
+    std::vector<double> pt(std::max<size_t>(nr * c.nham, 1), 0.0);
+    if (c.nham > 0) std::copy(g.ptab, g.ptab + nr * c.nham, pt.begin());
+    cudaError_t e;
+    if ((e = put_n(al, up, &dv, vlt.data(), vlt.size())) || (e = put_n(al, up, &di, ivt.data(), ivt.size())) ||
+        (e = put_n(al, up, &de, eint.data(), eint.size())) || (e = put_n(al, up, &dc, cent.data(), cent.size())) ||
+        (e = put_n(al, up, &drt, g.rtab, nr)) || (e = put_n(al, up, &dpt, pt.data(), pt.size())))
+        return set_err(MGPU_ERR_NOMEM, "uploading a system", e);
+    if (iprop == MGPU_PROP_LDMD && (e = alloc_n(al, &dq, (size_t)g.nstep * TT * nt)))
+        return set_err(MGPU_ERR_NOMEM, "allocating the 2HQ(C) table", e);
+    d.vlt = dv;
+    d.ivt = di;
+    d.eint = de;
+    d.cent = dc;
+    d.rtab = drt;
+    d.ptab = dpt;
+    d.q = dq;
+    return MGPU_OK;
+}
+
+constexpr int kPrepChunk = 128;  // U(C) steps inverted per preparation batch
+
+// Device state of one large-N bucket: M jobs (host copies `jobs`, device
+// `d_jobs`), and for MDPROP the U(C) descriptors of the systems `prep_sys`.
+// hs / sys_n / sys_nstep are indexed by the system ids the jobs carry;
+// d_prep points at the [3] counters of system 0.
+static int setup_big(BigBucket &g, int iprop, int b, const JobDev *jobs, const JobDev *d_jobs, int M, int max_nstep,
+                     const std::vector<int> &prep_sys, const std::vector<SysDev> &hs, const std::vector<int> &sys_n,
+                     const std::vector<int> &sys_nstep, int *d_prep, const AllocFn &al, const UploadFn &up)
+{
+    cudaError_t e;
+    const bool ldj = iprop == MGPU_PROP_LDJ;
+    g.b = b;
+    g.nt = kBuckets[b].nt;
+    g.npad = bucket_npad(b);
+    g.td = matrix_elems(b);
+    g.M = M;
+    g.d_jobs = d_jobs;
+    g.max_nstep = max_nstep;
+    if (M > 65535) return set_err(MGPU_ERR_UNSUPPORTED, "more than 65535 large-N propagations in one bucket");
+    int maxsteps = 0;
+    for (int sidx : prep_sys) maxsteps = std::max(maxsteps, sys_nstep[sidx]);
+    g.pcap = std::max({(ldj ? 2 : 1) * M, std::min(maxsteps, kPrepChunk), 1});
+    const size_t fr = (size_t)g.nt * big::MC * 32;  // doubles of one operand panel
+    int zero = 0;
+    if ((e = alloc_n(al, &g.pn[0].lam, (size_t)g.pcap * big::NB * big::NB)) ||
+        (e = alloc_n(al, &g.pn[0].rd, (size_t)g.pcap * big::NB)) || (e = alloc_n(al, &g.pn[0].xf, (size_t)g.pcap * fr)) ||
+        (e = alloc_n(al, &g.pn[0].bf, (size_t)g.pcap * fr)) || (e = alloc_n(al, &g.pn[1].xf, (size_t)g.pcap * fr)) ||
+        (e = alloc_n(al, &g.pn[1].bf, (size_t)g.pcap * fr)) || (e = put_n(al, up, &g.kstep, &zero, 1)) ||
+        (e = put_n(al, up, &g.kzero, &zero, 1)) ||
+        (M && ((e = alloc_n(al, &g.tiles, (size_t)M * g.td)) || (e = alloc_n(al, &g.ctr, (size_t)3 * M)) ||
+               (ldj && (e = alloc_n(al, &g.tiles2, (size_t)M * g.td))) ||
+               (!ldj && (e = alloc_n(al, &g.vec, (size_t)M * 3 * g.npad))))))
+        return set_err(MGPU_ERR_NOMEM, "allocating large-N matrices", e);
+    g.pn[1].lam = g.pn[0].lam;
+    g.pn[1].rd = g.pn[0].rd;
+    if (M) {
+        std::vector<big::MatDesc> md(M), uz;
+        for (int j = 0; j < M; ++j) {
+            big::MatDesc &d = md[j];
+            d.a = g.tiles + (size_t)j * g.td;
+            d.cnt = g.ctr + j;
+            d.stat = g.ctr + M + j;
+            d.kfail = g.ctr + 2 * M + j;
+            d.n = sys_n[jobs[j].sys];
+            d.sign = 1;
+            d.nstep = sys_nstep[jobs[j].sys];
+            d.kfix = 0;
+        }
+        if (ldj) {
+            uz = md;
+            for (int j = 0; j < M; ++j) {
+                uz[j].a = g.tiles2 + (size_t)j * g.td;
+                uz[j].sign = -1;
+            }
+            uz.insert(uz.end(), md.begin(), md.end());
+        }
+        if ((e = put_n(al, up, &g.d_md, md.data(), md.size())) ||
+            (ldj && (e = put_n(al, up, &g.d_mduz, uz.data(), uz.size()))))
+            return set_err(MGPU_ERR_NOMEM, "uploading large-N descriptors", e);
+    }
+    if (!ldj)
+        for (int sidx : prep_sys) {
+            const int ns = sys_nstep[sidx];
+            std::vector<big::MatDesc> md(ns);
+            for (int k = 1; k <= ns; ++k) {
+                big::MatDesc &d = md[k - 1];
+                d.a = hs[sidx].q + (size_t)(k - 1) * g.td;
+                d.cnt = d_prep + 3 * sidx;
+                d.stat = d_prep + 3 * sidx + 1;
+                d.kfail = d_prep + 3 * sidx + 2;
+                d.n = sys_n[sidx];
+                d.sign = 1;
+                d.nstep = 0x7fffffff;
+                d.kfix = k;
+            }
+            big::MatDesc *dm = nullptr;
+            if ((e = put_n(al, up, &dm, md.data(), md.size())))
+                return set_err(MGPU_ERR_NOMEM, "uploading preparation descriptors", e);
+            g.prep_sys.push_back(sidx);
+            g.prep_md.push_back(dm);
+        }
+    return MGPU_OK;
+}
+
+// MDPROP preparation of a large-N bucket's systems: U(C_k) for every step,
+// inverted in batches of steps, turned into 2HQ(C_k).
+static cudaError_t run_big_prep(const BigBucket &g, const SysDev *d_sys, const std::vector<int> &sys_nstep,
+                                cudaStream_t st, cudaStream_t side, cudaEvent_t evf, cudaEvent_t evj)
+{
+    cudaError_t e;
+    for (size_t i = 0; i < g.prep_sys.size(); ++i) {
+        const int s = g.prep_sys[i], ns = sys_nstep[s];
+        for (int k0 = 1; k0 <= ns; k0 += g.pcap) {
+            const int c = std::min(g.pcap, ns - k0 + 1);
+            const dim3 grid(big_ew_blocks(g.td), c);
+            big::big_prep_build_kernel<<<grid, big::EW_THREADS, 0, st>>>(d_sys, s, k0, g.td);
+            if ((e = big_invert(g.prep_md[i] + (k0 - 1), c, g.nt, g.pn, g.kzero, st, side, evf, evj))) return e;
+            big::big_prep_finish_kernel<<<grid, big::EW_THREADS, 0, st>>>(d_sys, s, k0, g.td);
+            if ((e = cudaGetLastError())) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+// The step loop of a large-N bucket: start, NSTEP x (elementwise, inversions),
+// results into y / nodes / status / kfail (indexed by JobDev::yoff / ::out).
+// `st` must not be the legacy default stream: one step (its ~4 x NT/8 x 2
+// launches, look-ahead fork/join included) is captured into a CUDA graph on
+// first use and replayed NSTEP times; the device-side step counter makes
+// every replay the next step.  The graph stays in g.step_graph for reuse.
+static cudaError_t run_big_prop(BigBucket &g, int iprop, const SysDev *d_sys, double *y, int *nodes, int *status,
+                                int *kfail, cudaStream_t st, cudaStream_t side, cudaEvent_t evf, cudaEvent_t evj)
+{
+    if (g.M == 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    const bool ldj = iprop == MGPU_PROP_LDJ;
+    big::StepArgs a{d_sys, g.d_jobs, g.d_md, g.tiles2, g.vec, g.kstep, g.npad, g.td};
+    const dim3 ew(big_ew_blocks(g.td), g.M), ev((g.npad + big::EW_THREADS - 1) / big::EW_THREADS, g.M);
+    auto one_step = [&]() -> cudaError_t {
+        cudaError_t x;
+        if (ldj) {
+            big::big_ldj_pre_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+            if ((x = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, g.kstep, st, side, evf, evj))) return x;  // U and Z
+            big::big_ldj_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+            if ((x = big_invert(g.d_md, g.M, g.nt, g.pn, g.kstep, st, side, evf, evj))) return x;
+            big::big_ldj_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+        } else {
+            big::big_ldmd_pre_kernel<<<ev, big::EW_THREADS, 0, st>>>(a);
+            if ((x = big_invert(g.d_md, g.M, g.nt, g.pn, g.kstep, st, side, evf, evj))) return x;
+            big::big_ldmd_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+            if ((x = big_invert(g.d_md, g.M, g.nt, g.pn, g.kstep, st, side, evf, evj))) return x;
+            big::big_ldmd_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
+        }
+        big::big_step_advance_kernel<<<1, 1, 0, st>>>(g.kstep, -1);
+        return cudaGetLastError();
+    };
+    if (!g.step_graph) {
+        cudaGraph_t graph = nullptr;
+        if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal))) return e;
+        const cudaError_t e1 = one_step();
+        const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+        if (e1 || e2) {
+            if (graph) cudaGraphDestroy(graph);
+            return e1 ? e1 : e2;
+        }
+        e = cudaGraphInstantiate(&g.step_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e) {
+            g.step_graph = nullptr;
+            return e;
+        }
+    }
+    big::big_step_advance_kernel<<<1, 1, 0, st>>>(g.kstep, 1);
+    if (ldj) big::big_ldj_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
+    else big::big_ldmd_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
+    for (int k = 1; k <= g.max_nstep; ++k)
+        if ((e = cudaGraphLaunch(g.step_graph, st))) return e;
+    big::big_finish_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, ldj ? 1 : 0, y, nodes, status, kfail);
+    return cudaGetLastError();
+}
+
+// the kernels' attributes (dynamic shared memory above 48 KB), once per device
+static cudaError_t big_kernel_attributes()
+{
+    cudaError_t e;
+    if ((e = set_smem(big::big_update_kernel, big::kUpdSmem)) || (e = set_smem(big::big_factor_kernel, big::kFactSmem)))
+        return e;
+    return cudaSuccess;
+}
 
 static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g, int iprop)
 {
@@ -1082,83 +1366,26 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     p->nsys = nsys;
     p->njobs = njobs;
 
+    const AllocFn sync_alloc = [p](void **q, size_t bytes) {
+        cudaError_t e = cudaMalloc(q, bytes);
+        if (e == cudaSuccess) p->allocs.push_back(*q);
+        return e;
+    };
+    const UploadFn sync_upload = [](void *dst, const void *src, size_t bytes) {
+        return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+    };
     std::vector<SysDev> hs(nsys);
     for (int s = 0; s < nsys; ++s) {
-        const mgpu_coupling &c = systems[s];
-        const mgpu_grid &g = grids[s];
-        const int b = bucket_for(c.n, iprop);
-        const int npad = bucket_npad(b);
-        const int nt = ntiles_of(b);
-        const size_t TT = tile_elems(b);
-        p->sys_n.push_back(c.n);
+        const int b = bucket_for(systems[s].n, iprop);
+        p->sys_n.push_back(systems[s].n);
         p->sys_bucket.push_back(b);
-        p->sys_nstep.push_back(g.nstep);
-        p->sys_nham.push_back(c.nham);
-        // VL / IV into the bucket's tile layout
-        const size_t tsz = (size_t)std::max(c.nham, 1) * TT * nt;
-        std::vector<double> vlt(tsz, 0.0);
-        std::vector<int> ivt(c.ivlfl > 0 ? tsz : 1, 0);
-        for (int t = 0; t < nt; ++t)
-            for (int ee = 0; ee < (int)TT; ++ee) {
-                int i = 0, j = 0;
-                tile_element(b, t, ee, &i, &j);
-                if (i >= c.n || j >= c.n) continue;
-                const int lo = std::min(i, j), hi = std::max(i, j);
-                // pair (row lo, column hi) of the packed upper triangle (sumlam.f:33-36,74-86)
-                const size_t pair = (size_t)hi * (hi + 1) / 2 + lo;
-                for (int l = 0; l < c.nham; ++l) {
-                    const size_t src = pair * c.nvlblk + l;
-                    const size_t dst = tile_offset(b, l, t, ee);
-                    vlt[dst] = c.vl[src];
-                    if (c.ivlfl > 0) {
-                        int ix = c.iv[src] - 1;
-                        if (ix < 0 || ix >= c.nham) {
-                            delete p;
-                            return set_err(MGPU_ERR_ARG, "IV index outside 1..NHAM");
-                        }
-                        ivt[dst] = ix;
-                    }
-                }
-            }
-        std::vector<double> eint(npad, 0.0), cent(npad, 0.0);
-        std::copy(c.eint, c.eint + c.n, eint.begin());
-        std::copy(c.cent, c.cent + c.n, cent.begin());
-        SysDev &d = hs[s];
-        memset(&d, 0, sizeof d);
-        d.n = c.n;
-        d.nham = c.nham;
-        d.ivlfl = c.ivlfl;
-        d.nconst = c.nconst;
-        d.nrsq = c.nrsq;
-        d.nstep = g.nstep;
-        d.ntiles = nt;
-        d.kind = frag_layout(b) ? 1 : 0;
-        d.conlen = c.conlen;
-        d.dr = g.dr;
-        const size_t nr = 2 * (size_t)g.nstep + 1;
-        double *dv = nullptr, *de = nullptr, *dc = nullptr, *drt = nullptr, *dpt = nullptr, *dq = nullptr;
-        int *di = nullptr;
-        std::vector<double> pt(std::max<size_t>(nr * c.nham, 1), 0.0);
-        if (c.nham > 0) std::copy(g.ptab, g.ptab + nr * c.nham, pt.begin());
-        if ((e = upload(p, &dv, vlt.data(), vlt.size())) || (e = upload(p, &di, ivt.data(), ivt.size())) ||
-            (e = upload(p, &de, eint.data(), eint.size())) || (e = upload(p, &dc, cent.data(), cent.size())) ||
-            (e = upload(p, &drt, g.rtab, nr)) || (e = upload(p, &dpt, pt.data(), pt.size()))) {
+        p->sys_nstep.push_back(grids[s].nstep);
+        p->sys_nham.push_back(systems[s].nham);
+        const int rc = build_sysdev(systems[s], grids[s], iprop, b, hs[s], sync_alloc, sync_upload);
+        if (rc) {
             delete p;
-            return set_err(MGPU_ERR_NOMEM, "uploading a system", e);
+            return rc;
         }
-        if (iprop == MGPU_PROP_LDMD) {
-            if ((e = p->dalloc(&dq, (size_t)g.nstep * TT * nt))) {
-                delete p;
-                return set_err(MGPU_ERR_NOMEM, "allocating the 2HQ(C) table", e);
-            }
-        }
-        d.vlt = dv;
-        d.ivt = di;
-        d.eint = de;
-        d.cent = dc;
-        d.rtab = drt;
-        d.ptab = dpt;
-        d.q = dq;
     }
     if (iprop == MGPU_PROP_LDMD)
         for (int s = 0; s < nsys; ++s) {
@@ -1237,105 +1464,34 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         return set_err(MGPU_ERR_NOMEM, "uploading jobs", e);
     }
     // large-N buckets: per-job tiled matrices and one round's scratch in device memory
-    constexpr int kPrepChunk = 128;  // U(C) steps inverted per preparation batch
     for (size_t slot = 0; slot < p->bucket_ids.size(); ++slot) {
         const int b = p->bucket_ids[slot];
         if (kBuckets[b].kind != KIND_BIG) continue;
         if (p->big.empty()) {
-            int zero[2] = {0, 0}, lo = 0, hi = 0;
+            int lo = 0, hi = 0;
             if ((e = cudaDeviceGetStreamPriorityRange(&lo, &hi)) ||
                 (e = cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, hi)) ||
+                (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)) ||
                 (e = cudaEventCreateWithFlags(&p->evf, cudaEventDisableTiming)) ||
                 (e = cudaEventCreateWithFlags(&p->evj, cudaEventDisableTiming)) ||
-                (e = upload(p, &p->d_kstep, zero, 1)) || (e = upload(p, &p->d_kzero, zero, 1)) ||
-                (e = set_smem(big::big_update_kernel, big::kUpdSmem)) ||
-                (e = set_smem(big::big_factor_kernel, big::kFactSmem))) {
+                (e = cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming)) ||
+                (e = cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming)) || (e = big_kernel_attributes())) {
                 delete p;
-                return set_err(MGPU_ERR_NOMEM, "large-N set-up", e);
+                return set_err(MGPU_ERR_CUDA, "large-N set-up", e);
             }
         }
-        mgpu_plan::Big g;
-        g.slot = (int)slot;
-        g.b = b;
-        g.nt = kBuckets[b].nt;
-        g.npad = bucket_npad(b);
-        g.td = matrix_elems(b);
-        g.M = p->job_count[slot];
-        g.max_nstep = p->max_nstep[slot];
-        const bool ldj = iprop == MGPU_PROP_LDJ;
-        if (g.M > 65535) {
+        std::vector<int> prep;
+        if (iprop == MGPU_PROP_LDMD)
+            for (int i = 0; i < p->sys_count[slot]; ++i) prep.push_back(syslist[p->sys_begin[slot] + i]);
+        BigBucket g;
+        const int rc = setup_big(g, iprop, b, hj.data() + p->job_begin[slot], p->d_jobs + p->job_begin[slot],
+                                 p->job_count[slot], p->max_nstep[slot], prep, hs, p->sys_n, p->sys_nstep, p->d_prep,
+                                 sync_alloc, sync_upload);
+        if (rc) {
             delete p;
-            return set_err(MGPU_ERR_UNSUPPORTED, "more than 65535 large-N propagations in one plan bucket");
+            return rc;
         }
-        int maxsteps = 0;
-        for (int i = 0; i < p->sys_count[slot]; ++i) maxsteps = std::max(maxsteps, p->sys_nstep[syslist[p->sys_begin[slot] + i]]);
-        g.pcap = std::max((ldj ? 2 : 1) * g.M, ldj ? 1 : std::min(maxsteps, kPrepChunk));
-        const size_t fr = (size_t)g.nt * big::MC * 32;  // doubles of one operand panel
-        if ((e = p->dalloc(&g.pn[0].lam, (size_t)g.pcap * big::NB * big::NB)) ||
-            (e = p->dalloc(&g.pn[0].rd, (size_t)g.pcap * big::NB)) || (e = p->dalloc(&g.pn[0].xf, (size_t)g.pcap * fr)) ||
-            (e = p->dalloc(&g.pn[0].bf, (size_t)g.pcap * fr)) || (e = p->dalloc(&g.pn[1].xf, (size_t)g.pcap * fr)) ||
-            (e = p->dalloc(&g.pn[1].bf, (size_t)g.pcap * fr)) ||
-            (g.M && ((e = p->dalloc(&g.tiles, (size_t)g.M * g.td)) || (e = p->dalloc(&g.ctr, (size_t)3 * g.M)) ||
-                     (ldj && (e = p->dalloc(&g.tiles2, (size_t)g.M * g.td))) ||
-                     (!ldj && (e = p->dalloc(&g.vec, (size_t)g.M * 3 * g.npad)))))) {
-            delete p;
-            return set_err(MGPU_ERR_NOMEM, "allocating large-N matrices", e);
-        }
-        g.pn[1].lam = g.pn[0].lam;
-        g.pn[1].rd = g.pn[0].rd;
-        if (g.M) {
-            std::vector<big::MatDesc> md(g.M), uz;
-            for (int j = 0; j < g.M; ++j) {
-                const JobDev &jd = hj[p->job_begin[slot] + j];
-                big::MatDesc &d = md[j];
-                d.a = g.tiles + (size_t)j * g.td;
-                d.cnt = g.ctr + j;
-                d.stat = g.ctr + g.M + j;
-                d.kfail = g.ctr + 2 * g.M + j;
-                d.n = p->sys_n[jd.sys];
-                d.sign = 1;
-                d.nstep = p->sys_nstep[jd.sys];
-                d.kfix = 0;
-            }
-            if (ldj) {
-                uz = md;
-                for (int j = 0; j < g.M; ++j) {
-                    uz[j].a = g.tiles2 + (size_t)j * g.td;
-                    uz[j].sign = -1;
-                }
-                uz.insert(uz.end(), md.begin(), md.end());
-            }
-            if ((e = upload(p, &g.d_md, md.data(), md.size())) ||
-                (ldj && (e = upload(p, &g.d_mduz, uz.data(), uz.size())))) {
-                delete p;
-                return set_err(MGPU_ERR_NOMEM, "uploading large-N descriptors", e);
-            }
-        }
-        if (!ldj)
-            for (int i = 0; i < p->sys_count[slot]; ++i) {
-                const int sidx = syslist[p->sys_begin[slot] + i];
-                const int ns = p->sys_nstep[sidx];
-                std::vector<big::MatDesc> md(ns);
-                for (int k = 1; k <= ns; ++k) {
-                    big::MatDesc &d = md[k - 1];
-                    d.a = hs[sidx].q + (size_t)(k - 1) * g.td;
-                    d.cnt = p->d_prep + 3 * sidx;
-                    d.stat = p->d_prep + 3 * sidx + 1;
-                    d.kfail = p->d_prep + 3 * sidx + 2;
-                    d.n = p->sys_n[sidx];
-                    d.sign = 1;
-                    d.nstep = 0x7fffffff;
-                    d.kfix = k;
-                }
-                big::MatDesc *dm = nullptr;
-                if ((e = upload(p, &dm, md.data(), md.size()))) {
-                    delete p;
-                    return set_err(MGPU_ERR_NOMEM, "uploading preparation descriptors", e);
-                }
-                g.prep_sys.push_back(sidx);
-                g.prep_md.push_back(dm);
-            }
-        p->big.push_back(g);
+        p->big.push_back(std::move(g));
     }
     *out = p;
     return MGPU_OK;
@@ -1368,47 +1524,20 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
             }
         }
     }
-    if (p->iprop == MGPU_PROP_LDMD && (phases & 1))
-        for (const auto &g : p->big)
-            for (size_t i = 0; i < g.prep_sys.size(); ++i) {
-                const int s = g.prep_sys[i], ns = p->sys_nstep[s];
-                for (int k0 = 1; k0 <= ns; k0 += g.pcap) {
-                    const int c = std::min(g.pcap, ns - k0 + 1);
-                    const dim3 grid(big_ew_blocks(g.td), c);
-                    big::big_prep_build_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
-                    if ((e = big_invert(g.prep_md[i] + (k0 - 1), c, g.nt, g.pn, p->d_kzero, st, p->side, p->evf, p->evj)))
-                        return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
-                    big::big_prep_finish_kernel<<<grid, big::EW_THREADS, 0, st>>>(p->d_sys, s, k0, g.td);
-                    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
-                }
-            }
-    for (const auto &g : p->big) {
-        if (!(phases & 2) || g.M == 0) continue;
-        const bool ldj = p->iprop == MGPU_PROP_LDJ;
-        big::StepArgs a{p->d_sys, p->d_jobs + p->job_begin[g.slot], g.d_md, g.tiles2, g.vec, p->d_kstep, g.npad, g.td};
-        const dim3 ew(big_ew_blocks(g.td), g.M), ev((g.npad + big::EW_THREADS - 1) / big::EW_THREADS, g.M);
-        big::big_step_advance_kernel<<<1, 1, 0, st>>>(p->d_kstep, 1);
-        if (ldj) big::big_ldj_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y_dev);
-        else big::big_ldmd_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y_dev);
-        for (int k = 1; k <= g.max_nstep; ++k) {
-            if (ldj) {
-                big::big_ldj_pre_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;  // U and Z
-                big::big_ldj_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
-                big::big_ldj_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-            } else {
-                big::big_ldmd_pre_kernel<<<ev, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
-                big::big_ldmd_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-                if ((e = big_invert(g.d_md, g.M, g.nt, g.pn, p->d_kstep, st, p->side, p->evf, p->evj))) break;
-                big::big_ldmd_post_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
-            }
-            big::big_step_advance_kernel<<<1, 1, 0, st>>>(p->d_kstep, -1);
-        }
-        if (e || (e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
-        big::big_finish_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, ldj ? 1 : 0, y_dev, nodes_dev, status_dev, kfail_dev);
-        if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
+    if (!p->big.empty()) {
+        // the large-N work runs on the plan's own stream, ordered after and before the caller's
+        if ((e = cudaEventRecord(p->ev_in, st)) || (e = cudaStreamWaitEvent(p->own, p->ev_in, 0)))
+            return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
+        if (p->iprop == MGPU_PROP_LDMD && (phases & 1))
+            for (const auto &g : p->big)
+                if ((e = run_big_prep(g, p->d_sys, p->sys_nstep, p->own, p->side, p->evf, p->evj)))
+                    return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
+        for (auto &g : p->big)
+            if ((phases & 2) && (e = run_big_prop(g, p->iprop, p->d_sys, y_dev, nodes_dev, status_dev, kfail_dev,
+                                                  p->own, p->side, p->evf, p->evj)))
+                return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
+        if ((e = cudaEventRecord(p->ev_out, p->own)) || (e = cudaStreamWaitEvent(st, p->ev_out, 0)))
+            return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
     }
     for (size_t b = 0; b < p->bucket_ids.size() && (phases & 2); ++b) {
         if (p->job_count[b] == 0 || kBuckets[p->bucket_ids[b]].kind == KIND_BIG) continue;
@@ -1425,6 +1554,10 @@ int mgpu_plan_run_host(mgpu_plan *p, double *y, int *nodes, int *status, int *kf
     if (p->njobs == 0) return MGPU_OK;
     if (!y || !nodes || !status || !kfail) return set_err(MGPU_ERR_ARG, "null host buffer");
     cudaError_t e;
+    // everything on the plan's own stream, waited for alone (no device-wide
+    // synchronisation: other threads may be capturing graphs meanwhile)
+    if (!p->own && (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)))
+        return set_err(MGPU_ERR_CUDA, "plan stream", e);
     if (p->y_cap < p->yelems) {
         if (p->d_y) cudaFree(p->d_y);
         p->d_y = nullptr;
@@ -1442,16 +1575,16 @@ int mgpu_plan_run_host(mgpu_plan *p, double *y, int *nodes, int *status, int *kf
             return set_err(MGPU_ERR_NOMEM, "output buffers", e);
         p->out_cap = p->njobs;
     }
-    if ((e = cudaMemcpy(p->d_y, y, p->yelems * sizeof(double), cudaMemcpyHostToDevice)))
+    if ((e = cudaMemcpyAsync(p->d_y, y, p->yelems * sizeof(double), cudaMemcpyHostToDevice, p->own)))
         return set_err(MGPU_ERR_CUDA, "copying Y to the device", e);
-    int rc = mgpu_plan_run_device(p, p->d_y, p->d_nodes, p->d_status, p->d_kfail, nullptr);
+    int rc = mgpu_plan_run_device(p, p->d_y, p->d_nodes, p->d_status, p->d_kfail, p->own);
     if (rc) return rc;
-    if ((e = cudaDeviceSynchronize())) return set_err(MGPU_ERR_CUDA, "propagation", e);
-    if ((e = cudaMemcpy(y, p->d_y, p->yelems * sizeof(double), cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(nodes, p->d_nodes, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(status, p->d_status, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost)))
+    if ((e = cudaMemcpyAsync(y, p->d_y, p->yelems * sizeof(double), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(nodes, p->d_nodes, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(status, p->d_status, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)))
         return set_err(MGPU_ERR_CUDA, "copying results to the host", e);
+    if ((e = cudaStreamSynchronize(p->own))) return set_err(MGPU_ERR_CUDA, "propagation", e);
     return MGPU_OK;
 }
 
@@ -1692,3 +1825,4 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
         return set_err(MGPU_ERR_CUDA, "launching ldmd_prop_kernel", e);
     return MGPU_OK;
 }
+#include "server.cuh"
