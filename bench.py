@@ -47,6 +47,17 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="batch", choices=["batch", "serve"],
+                    help="batch: the batched rotor workload (default); serve: the request server under "
+                         "Poisson arrivals of mixed-N solves")
+    ap.add_argument("--requests", type=int, default=3000, help="serve: requests in the timed stream")
+    ap.add_argument("--rate", type=float, default=20000.0, help="serve: Poisson arrival rate, requests/s")
+    ap.add_argument("--nmin", type=int, default=16)
+    ap.add_argument("--nmax", type=int, default=256)
+    ap.add_argument("--serve-nstep", type=int, default=1000, help="serve: steps per propagation")
+    ap.add_argument("--serve-systems", type=int, default=32)
+    ap.add_argument("--streams", type=int, default=4)
+    ap.add_argument("--plain-sample", type=int, default=24)
     return ap.parse_args()
 
 
@@ -269,10 +280,87 @@ def dominant_bucket(wl, lo=33, hi=40):
             np.array([wl.job_ered[j] for j in jobs]), [wl.job_y0[j] for j in jobs])
 
 
+def run_serve(args):
+    """Request server under a seeded Poisson stream of single MDPROP solves,
+    N log-uniform in [nmin, nmax] over a pool of dense synthetic systems
+    registered (device-resident, 2HQ(C) prepared) before the timed region.
+    Beside it, the plain one-solve-at-a-time GPU loop (mgpu_mdprop per
+    request: plan, preparation and propagation every call) on a sample of the
+    same requests."""
+    import math
+    import numpy as np
+    import torch
+    from molscat_b200.build import build
+    build()
+    from molscat_b200 import systems as S
+    from molscat_b200.propagators import propagate
+    from molscat_b200.serving import Server, latency_percentiles
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(20261203)
+    K = args.serve_systems
+    ns = np.exp(rng.uniform(math.log(args.nmin), math.log(args.nmax), K)).astype(int)
+    pool = [S.synthetic_system(int(n), args.serve_nstep, seed=1000 + k) for k, n in enumerate(ns)]
+    R = args.requests
+    pick = rng.integers(0, K, R)
+    de = rng.uniform(0.0, 10.0, R)
+    arrive = np.cumsum(rng.exponential(1.0 / args.rate, R))
+    srv = Server("LDMD", hbm_budget=48 << 30, streams=args.streams, max_batch=4096, max_systems=K)
+    ids = [srv.add_system(c, seg) for (c, seg, _, _) in pool]
+    for k in range(K):  # first use of every bucket's kernels
+        srv.submit(ids[k], pool[k][2], pool[k][3]).wait()
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    reqs = []
+    for i in range(R):
+        while time.perf_counter() - t0 < arrive[i]:
+            pass
+        k = int(pick[i])
+        reqs.append(srv.submit(ids[k], pool[k][2] + de[i], pool[k][3]))
+    for r in reqs:
+        r.wait()
+    clk = clocks.stop()
+    t_first = min(r.times()[0] for r in reqs)
+    t_last = max(r.times()[2] for r in reqs)
+    wall = t_last - t_first
+    work = float(sum(int(ns[int(k)]) ** 3 * args.serve_nstep for k in pick))
+    lat = latency_percentiles(reqs, (50, 90, 99))
+    # the plain loop on the first requests, and equality of their results
+    ns_plain = min(args.plain_sample, R)
+    same = True
+    tp = time.perf_counter()
+    for i in range(ns_plain):
+        k = int(pick[i])
+        c, seg, e, y0 = pool[k]
+        y, nodes = propagate("LDMD", c, seg, e + de[i], y0)
+        same = same and bool(np.array_equal(y, reqs[i].wait())) and nodes == reqs[i].nodes
+    tp = time.perf_counter() - tp
+    work_plain = float(sum(int(ns[int(pick[i])]) ** 3 * args.serve_nstep for i in range(ns_plain)))
+    srv.close()
+    line = {
+        "metric": "channel^3*steps/s (served single MDPROP solves, mixed N)", "value": work / wall,
+        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "solves_per_s": R / wall, "latency_s": lat,
+        "plain_loop": {"value": work_plain / tp, "unit": UNIT, "solves_per_s": ns_plain / tp,
+                       "sample": f"first {ns_plain} requests, mgpu_mdprop one at a time"},
+        "served_over_plain": (work / wall) / (work_plain / tp), "results_equal_plain": same,
+        "config": {"workload": f"Poisson arrivals {args.rate:.0f}/s, {R} requests, N log-uniform "
+                               f"{args.nmin}-{args.nmax} over {K} dense synthetic systems (NHAM 6), "
+                               f"{args.serve_nstep} steps each, energies jittered per request",
+                   "streams": args.streams, "hbm_budget_gb": 48,
+                   "registration": "systems registered and 2HQ(C) prepared before the timed region"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "serve":
+        run_serve(args)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

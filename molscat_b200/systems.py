@@ -233,3 +233,41 @@ def batched_workload(n_energies: int = 512, jmax: int = 80, seed: int = 20261203
     e = batched_energies(n_energies, seed)
     return _rotor_jobs(jt, [1, 2], e, f"rotor JTOT=0..{jmax} x 2 parities x {n_energies} energies, {nstep} steps",
                        nstep=nstep)
+
+
+def synthetic_system(n: int, nstep: int = 3000, seed: int = 0, nham: int = 6):
+    """A dense coupled-channel system of exactly N channels for timing large
+    and mixed N: NHAM Lennard-Jones 12-6 radial terms with seeded amplitudes
+    and minima (R in units of the mean minimum, energies in the reduced units
+    of the propagator), seeded symmetric couplings of every pair, thresholds
+    and L values.  Returns (Coupling, Segment, ERED, Y0) with Y0 the diagonal
+    WKB start of yinit.f:96-117."""
+    rng = np.random.default_rng(seed)
+    npair = n * (n + 1) // 2
+    # pairs in SUMLAM order (sumlam.f:74-86): column by column, row <= column
+    col = np.repeat(np.arange(n), np.arange(1, n + 1))
+    row = np.arange(npair) - col * (col + 1) // 2
+    diag = row == col
+    scale = 0.3 / math.sqrt(max(1.0, n / 32.0))
+    coef = rng.normal(0.0, scale, size=(npair, nham))
+    coef[diag, 0] = 1.0
+    coef[~diag, 0] = 0.0
+    coef[diag, 1:] *= 0.3
+    vl = np.ascontiguousarray(coef.ravel())
+    eint = np.sort(rng.uniform(0.0, 60.0, n))
+    lv = rng.integers(0, 30, n)
+    cent = (lv * (lv + 1)).astype(np.float64)
+    amp = np.concatenate([[200.0], rng.uniform(10.0, 60.0, nham - 1)])
+    rmin = rng.uniform(0.95, 1.05, nham)
+
+    def pvec(r: float) -> np.ndarray:
+        x = rmin / r
+        return amp * (x ** 12 - 2.0 * x ** 6)
+
+    r0, r1 = 0.8, 8.0
+    dr = (r1 - r0) / nstep
+    seg = Segment.build(r0, dr, nstep, lambda r: pvec(r), nham)
+    c = Coupling(n=n, nham=nham, vl=vl, eint=eint, cent=cent)
+    ered = float(rng.uniform(20.0, 80.0))
+    y0 = wkb_initial_y(c, seg.ptab[0], seg.rtab[0], ered)
+    return c, seg, ered, y0
