@@ -50,9 +50,12 @@ struct G {
 
 __host__ __device__ constexpr int tix(int I, int J) { return I * (I + 1) / 2 + J; }
 
+// Not volatile: the result registers carry every dependency, and leaving
+// the compiler free to schedule DMMAs between other work helps it overlap
+// them with the look-ahead factorisation.
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
