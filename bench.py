@@ -296,6 +296,8 @@ def run_serve(args):
     from molscat_b200.propagators import propagate
     from molscat_b200.serving import Server, latency_percentiles
     torch.cuda.set_device(0)
+    from molscat_b200 import autotune
+    tuned = autotune.apply(autotune.default_path("LDMD")) if os.path.exists(autotune.default_path("LDMD")) else 0
     rng = np.random.default_rng(20261203)
     K = args.serve_systems
     ns = np.exp(rng.uniform(math.log(args.nmin), math.log(args.nmax), K)).astype(int)
@@ -348,7 +350,8 @@ def run_serve(args):
                                f"{args.nmin}-{args.nmax} over {K} dense synthetic systems (NHAM 6), "
                                f"{args.serve_nstep} steps each, energies jittered per request",
                    "streams": args.streams, "hbm_budget_gb": 48,
-                   "registration": "systems registered and 2HQ(C) prepared before the timed region"},
+                   "registration": "systems registered and 2HQ(C) prepared before the timed region",
+                   "tuning": f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"},
         "clocks": clk,
     }
     print(json.dumps(line), flush=True)
@@ -386,7 +389,10 @@ def main():
     if dist:
         dist.barrier()
     from molscat_b200 import systems as S
+    from molscat_b200 import autotune
     from molscat_b200.propagators import Plan
+    tpath = autotune.default_path("LDMD")
+    tuned = autotune.apply(tpath) if os.path.exists(tpath) else 0
 
     t_setup = time.perf_counter()
     wl = S.batched_workload(n_energies=args.energies, jmax=args.jmax, seed=20261203 + rank)
@@ -523,7 +529,8 @@ def main():
                        "systems": len(wl.systems), "propagations_per_gpu": njobs,
                        "l2": "inputs larger than L2 (2HQ(C) tables %.1f GB)" % (plan.flops_prep and
                                                                                  sum(16 * (((s.n + 3) // 4) * ((s.n + 3) // 4 + 1) // 2) * 8 * 4000 for s in wl.systems) / 1e9),
-                       "parallelism": "independent batches per GPU (no collective)" if world > 1 else "1 GPU"},
+                       "parallelism": "independent batches per GPU (no collective)" if world > 1 else "1 GPU",
+                       "tuning": f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"},
             "solves_per_s": jobs_all / (ms * 1e-3),
             "flops_counted_per_s": plan.flops * world / (ms * 1e-3),
             "gpu_launches": plan.launches * args.steps,

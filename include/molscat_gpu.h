@@ -220,6 +220,15 @@ int mgpu_server_in_flight(mgpu_server *server, int *batches, int *queued, size_t
  * Affects plans created afterwards; returns the previous setting. */
 int mgpu_set_kernel_family(int family);
 
+/* Kernel family for plans and servers created afterwards, for propagator
+ * iprop (0 = both) and n_lo <= N <= n_hi -- the autotuner's per-bucket choice
+ * (molscat_b200/autotune.py): 0 = the default order (one warp for N <= 40,
+ * one CTA up to 200, batched large-N above), 1 = 4x4 register tiles
+ * (N <= 64), 2 = the batched large-N kernels (any N).  The latest call
+ * covering N wins; a family without a bucket for N falls back to the default.
+ * family < 0 clears the choices of iprop (0: all). */
+int mgpu_set_family_for_n(int iprop, int n_lo, int n_hi, int family);
+
 /* ---- diagnostics --------------------------------------------------------- */
 const char *mgpu_status_string(int status);
 const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */

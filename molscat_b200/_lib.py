@@ -46,7 +46,7 @@ EXPORTS = (
     "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
     "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc", "mgpu_set_kernel_family",
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
-    "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight",
+    "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
 )
 
 _lib = None
@@ -90,6 +90,7 @@ def load(path: str | None = None):
     L.mgpu_last_error.restype = ctypes.c_char_p
     L.mgpu_max_n.argtypes = []
     L.mgpu_set_kernel_family.argtypes = [ctypes.c_int]
+    L.mgpu_set_family_for_n.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
     ll = ctypes.c_longlong
     L.mgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]
@@ -109,6 +110,16 @@ def load(path: str | None = None):
 
 FAMILY_DMMA = 0
 FAMILY_TILE4 = 1
+FAMILY_BIG = 2
+
+
+def set_family_for_n(n_lo: int, n_hi: int, family: int, prop: str | None = None) -> None:
+    """Per-N kernel family for plans created afterwards, for one propagator
+    ("LDMD" / "LDJ") or both (None); family < 0 clears."""
+    iprop = 0 if prop is None else (MGPU_PROP_LDMD if prop == "LDMD" else MGPU_PROP_LDJ)
+    rc = load().mgpu_set_family_for_n(iprop, int(n_lo), int(n_hi), int(family))
+    if rc != 0:
+        raise ValueError(last_error())
 
 
 def set_kernel_family(family: int) -> int:

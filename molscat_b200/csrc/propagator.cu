@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int it
 
 // NT of the large-N buckets (matrices in global memory, 64 pivots a round):
 // N up to 1024 in steps of 64
-#define MGPU_BIG_BUCKETS(X) X(32) X(40) X(48) X(56) X(64) X(72) X(80) X(88) X(96) X(104) X(112) X(120) X(128)
+#define MGPU_BIG_BUCKETS(X) X(8) X(16) X(24) X(32) X(40) X(48) X(56) X(64) X(72) X(80) X(88) X(96) X(104) X(112) X(120) X(128)
 
 // KIND_FRAG8: one warp per matrix; KIND_CTA8: one CTA per matrix (same 8x8
 // fragment data layout); KIND_BIG: batched kernels over matrices held in
@@ -638,8 +638,34 @@ static bool bucket_allows(int b, int iprop)
 // Smallest bucket that holds N: the fragment kernels first, then the 4x4
 // register tiles; g_prefer_tile4 puts the 4x4 tiles first where they fit.
 static int g_prefer_tile4 = 0;
-static int bucket_for(int n, int iprop = MGPU_PROP_LDMD)
+
+// Per-N family choices (from the autotuner): 0 = the default order (one
+// warp, one CTA, batched large-N), 1 = 4x4 register tiles, 2 = batched
+// large-N kernels.  Consulted before the default order; a family that has no
+// bucket for N falls back to it.
+struct FamilyRange {
+    int iprop, lo, hi, family;  // iprop 0: both propagators
+};
+static std::vector<FamilyRange> g_family_ranges;
+static std::mutex g_family_mu;
+
+static int bucket_of_kind(int n, int iprop, int kind)
 {
+    for (int b = 0; b < kNumBuckets; ++b)
+        if (kBuckets[b].kind == kind && bucket_npad(b) >= n && bucket_allows(b, iprop)) return b;
+    return -1;
+}
+
+static int bucket_for(int n, int iprop = MGPU_PROP_LDMD, bool tuned = true)
+{
+    if (tuned) {
+        std::lock_guard<std::mutex> lk(g_family_mu);
+        for (const auto &r : g_family_ranges)
+            if ((r.iprop == 0 || r.iprop == iprop) && n >= r.lo && n <= r.hi && r.family != 0) {
+                const int b = bucket_of_kind(n, iprop, r.family == 1 ? KIND_TILE4 : KIND_BIG);
+                if (b >= 0) return b;
+            }
+    }
     for (int pass = 0; pass < 2; ++pass) {
         const bool tile4 = (pass == 0) == (g_prefer_tile4 != 0);
         for (int b = 0; b < kNumBuckets; ++b)
@@ -1269,6 +1295,22 @@ int mgpu_set_kernel_family(int family)
     return old;
 }
 
+int mgpu_set_family_for_n(int iprop, int n_lo, int n_hi, int family)
+{
+    std::lock_guard<std::mutex> lk(g_family_mu);
+    if (iprop != 0 && iprop != MGPU_PROP_LDMD && iprop != MGPU_PROP_LDJ)
+        return set_err(MGPU_ERR_ARG, "IPROP must be 0 (both), 5 or 6");
+    if (family < 0) {
+        g_family_ranges.erase(std::remove_if(g_family_ranges.begin(), g_family_ranges.end(),
+                                             [iprop](const FamilyRange &r) { return iprop == 0 || r.iprop == iprop; }),
+                              g_family_ranges.end());
+        return MGPU_OK;
+    }
+    if (family > 2 || n_lo < 1 || n_hi < n_lo) return set_err(MGPU_ERR_ARG, "family 0..2 and 1 <= n_lo <= n_hi");
+    g_family_ranges.insert(g_family_ranges.begin(), FamilyRange{iprop, n_lo, n_hi, family});  // latest wins
+    return MGPU_OK;
+}
+
 int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out)
 {
     if (!out_dev || iters < 1) return set_err(MGPU_ERR_ARG, "probe arguments");
@@ -1734,7 +1776,7 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
     if ((c->nham > 0 && (!c->vl || !g->ptab)) || (c->ivlfl > 0 && !c->iv) || !c->eint || !c->cent || !g->rtab ||
         !ered_dev || !y_dev || !nodes_dev || !status_dev || !kfail_dev)
         return set_err(MGPU_ERR_ARG, "null device pointer");
-    const int b = bucket_for(c->n);
+    const int b = bucket_for(c->n, MGPU_PROP_LDMD, false);  // the default order, whatever the tuning
     // the one-warp and one-CTA kernels only (N <= 200): the large-N kernels need per-job device matrices
     if (b < 0 || kBuckets[b].kind == KIND_BIG)
         return set_err(MGPU_ERR_UNSUPPORTED, "N above 200 (largest size of the allocation-free entry point)");

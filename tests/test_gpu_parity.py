@@ -214,3 +214,19 @@ def test_large_n_1024():
     yo, no, st, _ = oracle_prop("LDMD", c, seg, ered, y0)
     assert st == 0 and ng == no
     assert cases.rel_err(yg, yo) < Y_TOL
+
+
+@pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
+@pytest.mark.parametrize("n", [5, 36, 64, 100, 150])
+def test_batched_large_n_family_at_small_n(prop, n):
+    """The batched global-memory kernels selected for small N (the
+    autotuner's family 2; one to three 64-pivot rounds)."""
+    _lib.set_family_for_n(n, n, _lib.FAMILY_BIG)
+    try:
+        c, seg, ered, y0 = cases.random_case(n, 120, seed=4000 + n)
+        yg, ng = propagate(prop, c, seg, ered, y0)
+    finally:
+        _lib.set_family_for_n(-1, -1, -1)
+    yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
+    assert st == 0 and ng == no
+    assert cases.rel_err(yg, yo) < Y_TOL
