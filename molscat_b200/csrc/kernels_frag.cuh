@@ -194,11 +194,14 @@ ldmd_prep_frag_kernel(const SysDev *__restrict__ systems, const int *__restrict_
         }
 }
 
+// NT = 5 (N 33-40) is capped at 168 registers: three CTAs (12 warps) per SM
+// hide more of the per-round latency than the few spills cost (measured
+// +7 % at N = 36); smaller NT keep their natural register count.
 // ---------------------------------------------------------------------------
 // MDPROP step loop, one warp per job.
 // ---------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(32 * kWPB)
+__global__ void __launch_bounds__(32 * kWPB, NT >= 5 ? 3 : 1)
 ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs,
                       double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
                       int *__restrict__ kfail_out)
