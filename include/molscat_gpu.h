@@ -125,6 +125,27 @@ int mgpu_plan_run_device_phases(mgpu_plan *plan, double *y_dev, int *nodes_dev,
                                 int *status_dev, int *kfail_dev, void *stream,
                                 int phases);
 
+/* ---- Y -> K -> S on the device ---------------------------------------------
+ * YTOK/YTOKG/KSYM (ytok.f:21-47, ytokg.f:71-126) and KTOS (ktos.f:149-169)
+ * for every job after its propagation, at R = the grid's last radius: the
+ * Riccati-Bessel (open) and modified spherical Bessel (closed) boundary
+ * functions, K from Y by a pivoted linear solve, S = (I + iK)(I - iK)^{-1}.
+ * Channels in CHNSRT order (chnsrt.f:16-30: by threshold; the NOPEN open
+ * channels first).  S buffers hold, job after job, the NOPEN x NOPEN
+ * column-major real (SR) and imaginary (SI) parts.  Every system of the plan
+ * must have N <= 64 (else MGPU_ERR_UNSUPPORTED).  A job whose propagation
+ * failed keeps its status and gets no S; a singular K system sets status to
+ * MGPU_ERR_INVERSION. */
+size_t mgpu_plan_s_elems(const mgpu_plan *plan);          /* doubles in an SR (or SI) buffer */
+size_t mgpu_plan_s_offset(const mgpu_plan *plan, int job); /* first double of job's S */
+int mgpu_plan_nopen(const mgpu_plan *plan, int job);       /* open channels of job */
+/* device buffers: y_dev after a run, status_dev as the run left it */
+int mgpu_plan_smatrix_device(mgpu_plan *plan, const double *y_dev, double *sr_dev, double *si_dev,
+                             int *status_dev, void *stream);
+/* host buffers: initial Y in, S matrices and NODES / status / failing step out */
+int mgpu_plan_run_host_smatrix(mgpu_plan *plan, const double *y, double *sr, double *si, int *nodes,
+                               int *status, int *kfail);
+
 /* The number of kernel launches one run of the plan makes. */
 int mgpu_plan_launches(const mgpu_plan *plan);
 /* FP64 work the propagation phase alone does, and the LDMD preparation alone

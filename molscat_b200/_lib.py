@@ -47,6 +47,8 @@ EXPORTS = (
     "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc", "mgpu_set_kernel_family",
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
     "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
+    "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
+    "mgpu_plan_run_host_smatrix",
 )
 
 _lib = None
@@ -91,6 +93,13 @@ def load(path: str | None = None):
     L.mgpu_max_n.argtypes = []
     L.mgpu_set_kernel_family.argtypes = [ctypes.c_int]
     L.mgpu_set_family_for_n.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.mgpu_plan_s_elems.argtypes = [vp]
+    L.mgpu_plan_s_elems.restype = ctypes.c_size_t
+    L.mgpu_plan_s_offset.argtypes = [vp, ctypes.c_int]
+    L.mgpu_plan_s_offset.restype = ctypes.c_size_t
+    L.mgpu_plan_nopen.argtypes = [vp, ctypes.c_int]
+    L.mgpu_plan_smatrix_device.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.mgpu_plan_run_host_smatrix.argtypes = [vp, _dp, _dp, _dp, _ip, _ip, _ip]
     ll = ctypes.c_longlong
     L.mgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]

@@ -1,0 +1,250 @@
+// Y -> K -> S on the device (YTOK/YTOKG/KSYM ytok.f:21-47, ytokg.f:71-126;
+// KTOS ktos.f:149-169), one CTA per propagation, N <= 64 (the matrices live
+// in shared memory).  Included by propagator.cu.
+//
+// For channel i with wavevector w_i = sign(E - EINT_i) sqrt|E - EINT_i| and
+// L from CENT_i = L(L+1), at R = the grid's last radius:
+//   open   (E > EINT):  sj = x j_L(x)/sqrt(w), sjp = (x j_L)'(x) sqrt(w),
+//                       sn = x y_L(x)/sqrt(w), snp = (x y_L)'(x) sqrt(w),  x = w R
+//   closed:             sn = 1, snp = |w| d/dx ln[x k_L(x)],  x = |w| R
+// In channel order NB (CHNSRT: open channels first, by threshold), with
+// KM = Y diag(sn) - diag(snp) and T = Y[:, open] diag(sj) - diag(sjp), the
+// K matrix is the open block of KM^{-1} T, symmetrised, and
+//   S = (I + iK)(I - iK)^{-1}:  SR = 2(I + K^2)^{-1} - I,  SI = 2(I + K^2)^{-1} K.
+// The spherical Bessel functions come from their standard three-term
+// recurrences (y_L upward; j_L upward while L < x, otherwise Miller's downward
+// recurrence normalised by j_0 or j_1; k_L upward in its scaled form).
+#pragma once
+
+namespace mgpu {
+namespace smx {
+
+constexpr int kMaxN = 64;
+constexpr int kThreads = 128;
+// dynamic shared memory: [KM | T] with padded rows, then K
+__host__ __device__ constexpr size_t smem_bytes(int n, int no) { return ((size_t)n * (n + no + 1) + (size_t)no * no) * 8; }
+
+struct SJob {
+    int sys;         // system index
+    int nopen;       // open channels
+    int out;         // index in the caller's order (status, Y offset)
+    int pad;
+    double ered;
+    long long yoff;  // first double of the job's Y
+    long long soff;  // first double of the job's SR / SI
+};
+
+// x j_L, (x j_L)', x y_L, (x y_L)'
+__device__ void riccati(int l, double x, double &uj, double &ujp, double &un, double &unp)
+{
+    double s, c;
+    sincos(x, &s, &c);
+    // y: upward from y_{-1} = sin x / x, y_0 = -cos x / x
+    double yprev = s / x, ycur = -c / x;
+    for (int m = 0; m < l; ++m) {
+        const double t = (2 * m + 1) / x * ycur - yprev;
+        yprev = ycur;
+        ycur = t;
+    }
+    double jl, jlm1;
+    if (l < x) {
+        double jprev = c / x, jcur = s / x;  // j_{-1}, j_0
+        for (int m = 0; m < l; ++m) {
+            const double t = (2 * m + 1) / x * jcur - jprev;
+            jprev = jcur;
+            jcur = t;
+        }
+        jl = jcur;
+        jlm1 = jprev;
+    } else {
+        const int L = (int)fmax((double)l, x) + 40;
+        double fp1 = 0.0, f = 1e-280, f1 = 0.0;
+        jl = jlm1 = 0.0;
+        for (int m = L; m > 0; --m) {
+            const double fm1 = (2 * m + 1) / x * f - fp1;
+            if (m == l) {
+                jl = f;
+                jlm1 = fm1;
+            }
+            if (m == 1) f1 = f;
+            fp1 = f;
+            f = fm1;
+            if (fabs(f) > 1e250) {
+                fp1 *= 1e-250;
+                f *= 1e-250;
+                jl *= 1e-250;
+                jlm1 *= 1e-250;
+                f1 *= 1e-250;
+            }
+        }
+        const double j0 = s / x, j1 = s / (x * x) - c / x;
+        const double scale = fabs(j0) > fabs(j1) ? j0 / f : j1 / f1;
+        jl *= scale;
+        jlm1 *= scale;
+        if (l == 0) jlm1 = c / x;
+    }
+    uj = x * jl;
+    un = x * ycur;
+    ujp = x * jlm1 - l * jl;
+    unp = x * yprev - l * ycur;
+}
+
+// d/dx ln[x k_L(x)] from the scaled recurrence k_{-1} = k_0, k_{m+1} = k_{m-1} + (2m+1)/x k_m
+__device__ double klogd(int l, double x)
+{
+    double kprev = 1.0 / x, kcur = 1.0 / x;
+    for (int m = 0; m < l; ++m) {
+        const double t = kprev + (2 * m + 1) / x * kcur;
+        kprev = kcur;
+        kcur = t;
+    }
+    return -kprev / kcur - l / x;
+}
+
+// Gauss-Jordan on the first `nr` rows of A (row stride lda): columns [0, nr)
+// are reduced to I, columns [nr, ncol) become A^{-1} B.  Partial pivoting when
+// `pivot`.  Returns false (all threads) on a zero pivot.
+__device__ bool gauss_jordan(double *A, int lda, int nr, int ncol, bool pivot, int *s_p, double *s_f)
+{
+    const int tid = threadIdx.x;
+    for (int k = 0; k < nr; ++k) {
+        if (pivot && tid < 32) {
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + tid; i < nr; i += 32) {
+                const double v = fabs(A[i * lda + k]);
+                if (v > best) {
+                    best = v;
+                    bi = i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (tid == 0) *s_p = bi;
+        }
+        __syncthreads();
+        const int p = pivot ? *s_p : k;
+        if (p != k)
+            for (int j = tid; j < ncol; j += kThreads) {
+                const double t = A[k * lda + j];
+                A[k * lda + j] = A[p * lda + j];
+                A[p * lda + j] = t;
+            }
+        __syncthreads();
+        const double piv = A[k * lda + k];
+        if (piv == 0.0 || !isfinite(piv)) return false;
+        const double rp = 1.0 / piv;
+        for (int j = k + 1 + tid; j < ncol; j += kThreads) A[k * lda + j] *= rp;
+        if (tid < nr) s_f[tid] = A[tid * lda + k];
+        __syncthreads();
+        if (tid == 0) A[k * lda + k] = 1.0;
+        const int w = ncol - k - 1;
+        for (int e = tid; e < nr * w; e += kThreads) {
+            const int i = e / w, j = k + 1 + e % w;
+            if (i != k) A[i * lda + j] = fma(-s_f[i], A[k * lda + j], A[i * lda + j]);
+        }
+        for (int i = tid; i < nr; i += kThreads)
+            if (i != k) A[i * lda + k] = 0.0;
+        __syncthreads();
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kThreads)
+smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs, const int *__restrict__ nb_all,
+               const int *__restrict__ nb_off, const double *__restrict__ y, double *__restrict__ sr,
+               double *__restrict__ si, int *__restrict__ status)
+{
+    extern __shared__ __align__(16) double smx_sm[];
+    __shared__ double sj[kMaxN], sjp[kMaxN], sn[kMaxN], snp[kMaxN], s_f[kMaxN];
+    __shared__ int s_nb[kMaxN], s_p;
+    const SJob job = jobs[blockIdx.x];
+    const SysDev &S = systems[job.sys];
+    const int n = S.n, no = job.nopen, tid = threadIdx.x;
+    if (status[job.out] != MGPU_OK || no == 0) return;  // the propagation failed, or no open channel: no S
+    const int lda = n + no + 1;
+    double *A = smx_sm;                      // n x (n + no): [KM | T]
+    double *K = smx_sm + (size_t)n * lda;    // no x no
+    const double R = S.rtab[2 * S.nstep];
+    for (int c = tid; c < n; c += kThreads) {
+        s_nb[c] = nb_all[nb_off[job.sys] + c];
+        const double dif = job.ered - S.eint[c];
+        const double w = copysign(sqrt(fabs(dif)), dif);
+        const int ell = (int)lrint(sqrt(S.cent[c] + 0.25) - 0.5);
+        if (dif > 0.0) {
+            double uj, ujp, un, unp;
+            riccati(ell, w * R, uj, ujp, un, unp);
+            const double rd = sqrt(w);
+            sj[c] = uj / rd;
+            sjp[c] = ujp * rd;
+            sn[c] = un / rd;
+            snp[c] = unp * rd;
+        } else {
+            const double aw = fabs(w);
+            sj[c] = sjp[c] = 0.0;
+            sn[c] = 1.0;
+            snp[c] = klogd(ell, aw * R) * aw;
+        }
+    }
+    __syncthreads();
+    const double *yj = y + job.yoff;
+    for (int e = tid; e < n * (n + no); e += kThreads) {
+        const int i = e / (n + no), j = e % (n + no);
+        const int a = s_nb[i];
+        if (j < n) {
+            const int b = s_nb[j];
+            A[i * lda + j] = yj[a + (size_t)b * n] * sn[b] - (i == j ? snp[a] : 0.0);
+        } else {
+            const int b = s_nb[j - n];
+            A[i * lda + j] = yj[a + (size_t)b * n] * sj[b] - (i == j - n ? sjp[a] : 0.0);
+        }
+    }
+    __syncthreads();
+    bool ok = gauss_jordan(A, lda, n, n + no, true, &s_p, s_f);
+    // K = symmetrised open block of KM^{-1} T
+    if (ok) {
+        for (int e = tid; e < no * no; e += kThreads) {
+            const int i = e / no, j = e % no;
+            K[i * no + j] = 0.5 * (A[i * lda + n + j] + A[j * lda + n + i]);
+        }
+        __syncthreads();
+        // [0.5 K K + 0.5 I | I] in the first `no` rows of A, then Gauss-Jordan (I + K^2 is positive definite)
+        for (int e = tid; e < no * 2 * no; e += kThreads) {
+            const int i = e / (2 * no), j = e % (2 * no);
+            double v;
+            if (j < no) {
+                v = 0.0;
+                for (int m = 0; m < no; ++m) v = fma(K[i * no + m], K[m * no + j], v);
+                v = 0.5 * v + (i == j ? 0.5 : 0.0);
+            } else {
+                v = (i == j - no) ? 1.0 : 0.0;
+            }
+            A[i * lda + j] = v;
+        }
+        __syncthreads();
+        ok = gauss_jordan(A, lda, no, 2 * no, false, &s_p, s_f);
+    }
+    if (!ok) {
+        if (tid == 0) status[job.out] = MGPU_ERR_INVERSION;
+        return;
+    }
+    // SR = SRINV - I, SI = SRINV K (column-major, channel order NB)
+    double *srj = sr + job.soff, *sij = si + job.soff;
+    for (int e = tid; e < no * no; e += kThreads) {
+        const int i = e % no, j = e / no;
+        const double inv = A[i * lda + no + j];
+        double v = 0.0;
+        for (int m = 0; m < no; ++m) v = fma(A[i * lda + no + m], K[m * no + j], v);
+        srj[e] = inv - (i == j ? 1.0 : 0.0);
+        sij[e] = v;
+    }
+}
+
+}  // namespace smx
+}  // namespace mgpu

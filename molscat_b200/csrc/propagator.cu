@@ -550,6 +550,7 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
 #include "kernels_frag.cuh"
 #include "kernels_cta.cuh"
 #include "kernels_big.cuh"
+#include "kernels_smatrix.cuh"
 namespace mgpu {
 
 __global__ void prep_reset_kernel(int *prep, int nsys)
@@ -946,6 +947,16 @@ struct mgpu_plan {
     std::vector<int> bucket_ids, job_begin, job_count, sys_begin, sys_count, max_nstep, vl_smem;
     std::vector<size_t> smem;
     std::vector<BigBucket> big;            // large-N buckets (KIND_BIG)
+    // Y -> S on the device (every system N <= 64): channel order NB per system, NOPEN and S offsets per job
+    bool s_ok = false;
+    std::vector<int> nopen;
+    std::vector<size_t> soff;
+    size_t selems = 0;
+    size_t s_smem = 0;
+    smx::SJob *d_sjobs = nullptr;
+    int *d_nb = nullptr, *d_nb_off = nullptr;
+    double *d_sr = nullptr, *d_si = nullptr;
+    size_t s_cap = 0;
     cudaStream_t side = nullptr;           // look-ahead stream of the large-N inversions
     cudaStream_t own = nullptr;            // the large-N work (never the legacy stream: graph capture)
     cudaEvent_t evf = nullptr, evj = nullptr, ev_in = nullptr, ev_out = nullptr;
@@ -971,6 +982,8 @@ struct mgpu_plan {
         if (d_nodes) cudaFree(d_nodes);
         if (d_status) cudaFree(d_status);
         if (d_kfail) cudaFree(d_kfail);
+        if (d_sr) cudaFree(d_sr);
+        if (d_si) cudaFree(d_si);
     }
     template <class X>
     cudaError_t dalloc(X **p, size_t count)
@@ -1535,6 +1548,54 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         }
         p->big.push_back(std::move(g));
     }
+    // channel order (CHNSRT, chnsrt.f:16-30: by threshold, equal thresholds keep
+    // their order), open channels and S offsets, for the device S matrix
+    p->nopen.resize(njobs);
+    p->soff.resize(njobs);
+    {
+        bool ok = true;
+        std::vector<int> nb_all, nb_off(nsys);
+        for (int s = 0; s < nsys; ++s) {
+            const mgpu_coupling &c = systems[s];
+            ok = ok && c.n <= smx::kMaxN;
+            nb_off[s] = (int)nb_all.size();
+            std::vector<int> nb(c.n);
+            for (int i = 0; i < c.n; ++i) nb[i] = i;
+            for (int i = 0; i + 1 < c.n; ++i)
+                for (int j = i + 1; j < c.n; ++j) {
+                    const double a = c.eint[nb[i]], bb = c.eint[nb[j]];
+                    if (a <= bb || std::fabs(a - bb) < 1.0e-11) continue;
+                    std::swap(nb[i], nb[j]);
+                }
+            nb_all.insert(nb_all.end(), nb.begin(), nb.end());
+        }
+        std::vector<smx::SJob> sj(njobs);
+        size_t so = 0;
+        for (int j = 0; j < njobs; ++j) {
+            const mgpu_coupling &c = systems[job_sys[j]];
+            int no = 0;
+            for (int i = 0; i < c.n; ++i) no += (job_ered[j] - c.eint[i] > 0.0) ? 1 : 0;
+            p->nopen[j] = no;
+            p->soff[j] = so;
+            so += (size_t)no * no;
+            sj[j].sys = job_sys[j];
+            sj[j].nopen = no;
+            sj[j].out = j;
+            sj[j].pad = 0;
+            sj[j].ered = job_ered[j];
+            sj[j].yoff = (long long)p->yoff[j];
+            sj[j].soff = (long long)p->soff[j];
+            p->s_smem = std::max(p->s_smem, smx::smem_bytes(c.n, no));
+        }
+        p->selems = so;
+        p->s_ok = ok;
+        if (ok && njobs > 0 &&
+            ((e = upload(p, &p->d_sjobs, sj.data(), sj.size())) || (e = upload(p, &p->d_nb, nb_all.data(), nb_all.size())) ||
+             (e = upload(p, &p->d_nb_off, nb_off.data(), nb_off.size())))) {
+            delete p;
+            return set_err(MGPU_ERR_NOMEM, "uploading S-matrix descriptors", e);
+        }
+    }
     *out = p;
     return MGPU_OK;
 }
@@ -1622,6 +1683,80 @@ int mgpu_plan_run_host(mgpu_plan *p, double *y, int *nodes, int *status, int *kf
     int rc = mgpu_plan_run_device(p, p->d_y, p->d_nodes, p->d_status, p->d_kfail, p->own);
     if (rc) return rc;
     if ((e = cudaMemcpyAsync(y, p->d_y, p->yelems * sizeof(double), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(nodes, p->d_nodes, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(status, p->d_status, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaMemcpyAsync(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)))
+        return set_err(MGPU_ERR_CUDA, "copying results to the host", e);
+    if ((e = cudaStreamSynchronize(p->own))) return set_err(MGPU_ERR_CUDA, "propagation", e);
+    return MGPU_OK;
+}
+
+size_t mgpu_plan_s_elems(const mgpu_plan *p) { return p ? p->selems : 0; }
+
+size_t mgpu_plan_s_offset(const mgpu_plan *p, int job)
+{
+    return (p && job >= 0 && job < p->njobs) ? p->soff[job] : 0;
+}
+
+int mgpu_plan_nopen(const mgpu_plan *p, int job) { return (p && job >= 0 && job < p->njobs) ? p->nopen[job] : -1; }
+
+int mgpu_plan_smatrix_device(mgpu_plan *p, const double *y_dev, double *sr_dev, double *si_dev, int *status_dev,
+                             void *stream)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 64 in every system");
+    if (p->njobs == 0 || p->selems == 0) return MGPU_OK;
+    if (!y_dev || !sr_dev || !si_dev || !status_dev) return set_err(MGPU_ERR_ARG, "null device buffer");
+    cudaError_t e;
+    if ((e = set_smem(smx::smatrix_kernel, p->s_smem))) return set_err(MGPU_ERR_CUDA, "S-matrix kernel set-up", e);
+    smx::smatrix_kernel<<<p->njobs, smx::kThreads, p->s_smem, (cudaStream_t)stream>>>(
+        p->d_sys, p->d_sjobs, p->d_nb, p->d_nb_off, y_dev, sr_dev, si_dev, status_dev);
+    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the S-matrix kernel", e);
+    return MGPU_OK;
+}
+
+int mgpu_plan_run_host_smatrix(mgpu_plan *p, const double *y, double *sr, double *si, int *nodes, int *status,
+                               int *kfail)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 64 in every system");
+    if (p->njobs == 0) return MGPU_OK;
+    if (!y || !nodes || !status || !kfail || (p->selems && (!sr || !si))) return set_err(MGPU_ERR_ARG, "null host buffer");
+    cudaError_t e;
+    if (!p->own && (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)))
+        return set_err(MGPU_ERR_CUDA, "plan stream", e);
+    if (p->y_cap < p->yelems) {
+        if (p->d_y) cudaFree(p->d_y);
+        p->d_y = nullptr;
+        if ((e = cudaMalloc(&p->d_y, p->yelems * sizeof(double)))) return set_err(MGPU_ERR_NOMEM, "Y buffer", e);
+        p->y_cap = p->yelems;
+    }
+    if (p->out_cap < p->njobs) {
+        if (p->d_nodes) cudaFree(p->d_nodes);
+        if (p->d_status) cudaFree(p->d_status);
+        if (p->d_kfail) cudaFree(p->d_kfail);
+        p->d_nodes = p->d_status = p->d_kfail = nullptr;
+        if ((e = cudaMalloc(&p->d_nodes, p->njobs * sizeof(int))) ||
+            (e = cudaMalloc(&p->d_status, p->njobs * sizeof(int))) ||
+            (e = cudaMalloc(&p->d_kfail, p->njobs * sizeof(int))))
+            return set_err(MGPU_ERR_NOMEM, "output buffers", e);
+        p->out_cap = p->njobs;
+    }
+    if (p->s_cap < p->selems) {
+        if (p->d_sr) cudaFree(p->d_sr);
+        if (p->d_si) cudaFree(p->d_si);
+        p->d_sr = p->d_si = nullptr;
+        if ((e = cudaMalloc(&p->d_sr, p->selems * sizeof(double))) || (e = cudaMalloc(&p->d_si, p->selems * sizeof(double))))
+            return set_err(MGPU_ERR_NOMEM, "S buffers", e);
+        p->s_cap = p->selems;
+    }
+    if ((e = cudaMemcpyAsync(p->d_y, y, p->yelems * sizeof(double), cudaMemcpyHostToDevice, p->own)))
+        return set_err(MGPU_ERR_CUDA, "copying Y to the device", e);
+    int rc = mgpu_plan_run_device(p, p->d_y, p->d_nodes, p->d_status, p->d_kfail, p->own);
+    if (!rc) rc = mgpu_plan_smatrix_device(p, p->d_y, p->d_sr, p->d_si, p->d_status, p->own);
+    if (rc) return rc;
+    if ((p->selems && ((e = cudaMemcpyAsync(sr, p->d_sr, p->selems * sizeof(double), cudaMemcpyDeviceToHost, p->own)) ||
+                       (e = cudaMemcpyAsync(si, p->d_si, p->selems * sizeof(double), cudaMemcpyDeviceToHost, p->own)))) ||
         (e = cudaMemcpyAsync(nodes, p->d_nodes, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
         (e = cudaMemcpyAsync(status, p->d_status, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
         (e = cudaMemcpyAsync(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)))

@@ -252,6 +252,35 @@ class Plan:
         n = self.systems[self.job_sys[j]].n
         return buf[self.offsets[j]:self.offsets[j] + n * n].reshape((n, n), order="F")
 
+    def nopen(self, j: int) -> int:
+        """Open channels of job j (ERED above the threshold)."""
+        return int(_lib.load().mgpu_plan_nopen(self._handle, int(j)))
+
+    def run_host_smatrix(self, ybuf: np.ndarray):
+        """Host Y in; the propagation, then Y -> K -> S on the device.  Returns
+        (SR buffer, SI buffer, NODES, status, kfail); unpack_s gives job j's
+        NOPEN x NOPEN matrices in CHNSRT channel order."""
+        L = _lib.load()
+        nj = self.njobs
+        ns = int(L.mgpu_plan_s_elems(self._handle))
+        y = np.ascontiguousarray(ybuf, dtype=np.float64)
+        sr = np.zeros(max(ns, 1))
+        si = np.zeros(max(ns, 1))
+        nodes = np.zeros(nj, dtype=np.int32)
+        status = np.zeros(nj, dtype=np.int32)
+        kfail = np.zeros(nj, dtype=np.int32)
+        rc = L.mgpu_plan_run_host_smatrix(self._handle, y.ctypes.data_as(_dp), sr.ctypes.data_as(_dp),
+                                          si.ctypes.data_as(_dp), nodes.ctypes.data_as(_ip),
+                                          status.ctypes.data_as(_ip), kfail.ctypes.data_as(_ip))
+        if rc != 0:
+            raise PropagatorError(f"run (S): {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+        return sr, si, nodes, status, kfail
+
+    def unpack_s(self, buf: np.ndarray, j: int) -> np.ndarray:
+        no = self.nopen(j)
+        off = int(_lib.load().mgpu_plan_s_offset(self._handle, int(j)))
+        return buf[off:off + no * no].reshape((no, no), order="F")
+
     def run_host(self, ybuf: np.ndarray):
         """Host buffers in and out.  Returns (Y buffer, NODES, status, kfail)."""
         L = _lib.load()
