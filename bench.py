@@ -462,19 +462,21 @@ def main():
     else:
         work_all, jobs_all = work, float(njobs)
 
-    # end to end through the C ABI with host buffers (H2D of initial Y, D2H of Y/NODES/status)
+    # end to end through the C ABI with host buffers: initial Y in, the
+    # propagation and Y -> K -> S on the device, S matrices, NODES, status out
     e2e = None
     if not args.no_e2e:
-        import ctypes
         k2 = args.e2e_steps or args.steps
-        plan.run_host(y0_host)  # warm
+        plan.run_host_smatrix(y0_host)  # warm
         times = []
+        s_elems = 0
         for _ in range(k2):
             if dist:
                 dist.barrier()
             ta = time.perf_counter()
-            yh, nd, stt, kf = plan.run_host(y0_host)
+            sr, si, nd, stt, kf = plan.run_host_smatrix(y0_host)
             times.append(time.perf_counter() - ta)
+            s_elems = sr.size
             if (stt != 0).any():
                 raise RuntimeError("e2e propagation failed")
         tm = statistics.mean(times)
@@ -483,8 +485,8 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             tm = float(t.item())
         e2e = {"value": work_all / tm, "unit": UNIT, "h2d_bytes_per_step": int(plan.y_elems * 8),
-               "d2h_bytes_per_step": int(plan.y_elems * 8 + 3 * 4 * njobs), "solves_per_s": jobs_all / tm,
-               "api": "mgpu_plan_run_host (C ABI, host buffers)"}
+               "d2h_bytes_per_step": int(2 * s_elems * 8 + 3 * 4 * njobs), "solves_per_s": jobs_all / tm,
+               "api": "mgpu_plan_run_host_smatrix (C ABI, host buffers; S matrices computed on the device)"}
 
     # the dominant kernel alone: the N 33-40 bucket's step launch, timed with
     # CUDA events on the stream it is launched on (prep run once before)
