@@ -194,14 +194,17 @@ ldmd_prep_frag_kernel(const SysDev *__restrict__ systems, const int *__restrict_
         }
 }
 
-// NT = 5 (N 33-40) is capped at 168 registers: three CTAs (12 warps) per SM
-// hide more of the per-round latency than the few spills cost (measured
-// +7 % at N = 36); smaller NT keep their natural register count.
+// Resident CTAs per SM the register budget is set for: NT = 5 (N 33-40) is
+// capped at 168 registers, three CTAs (12 warps) per SM hiding more of the
+// per-round latency than its few spills cost (+7 % at N = 36); the smaller NT
+// keep the occupancy their natural register counts give (an unconstrained
+// bound lets the compiler spend registers and lose a CTA per SM).
+constexpr int frag_min_blocks(int nt) { return nt <= 1 ? 5 : (nt <= 3 ? 4 : 3); }
 // ---------------------------------------------------------------------------
 // MDPROP step loop, one warp per job.
 // ---------------------------------------------------------------------------
 template <int NT>
-__global__ void __launch_bounds__(32 * kWPB, NT >= 5 ? 3 : 1)
+__global__ void __launch_bounds__(32 * kWPB, frag_min_blocks(NT))
 ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs,
                       double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
                       int *__restrict__ kfail_out)
