@@ -1,0 +1,133 @@
+"""Bound states by node counting (the BOUND search of bd.driver.f over the
+BDCTRL matching of bdctrl.f), with the propagations batched on the GPU.
+
+At energy E a system is propagated outward from RMIN to RMATCH and inward
+from RMAX to RMATCH (BDPSET's two segments, bdpset.f:26-44).  The number of
+bound states below E is
+
+    NODES_out + NODES_in + #{eigenvalues of Y_out(RMATCH) - Y_in(RMATCH) <= 0}
+
+(bdctrl.f:197,221-257): the propagators' negative-pivot counts plus the
+matching matrix's non-positive eigenvalues.  A state with node count k lies
+where that count steps from k to k+1; bisection on E (bd.driver.f:993-1054)
+brackets it, every state's trial energy going into one batched plan per
+round, so one GPU launch set serves all states.  The matching step is an N x
+N symmetric eigenvalue count on the host (the propagation is the cost).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Callable
+
+import numpy as np
+
+from .propagators import Coupling, Plan, Segment
+
+
+def w_matrix(c: Coupling, r: float, p: np.ndarray, ered: float) -> np.ndarray:
+    """W(R) of HAMMAT/SUMLAM (hammat.f:85-113, sumlam.f:74-86) on the host,
+    for the initial log-derivative matrices."""
+    n = c.n
+    npair = n * (n + 1) // 2
+    col = np.repeat(np.arange(n), np.arange(1, n + 1))
+    row = np.arange(npair) - col * (col + 1) // 2
+    blk = c.vl[:npair * c.nvlblk].reshape(npair, c.nvlblk)[:, :c.nham]
+    if c.ivlfl > 0:
+        idx = c.iv[:npair * c.nvlblk].reshape(npair, c.nvlblk)[:, :c.nham] - 1
+        vals = np.sum(blk * p[idx], axis=1)
+    else:
+        vals = blk @ p[:c.nham]
+    w = np.zeros((n, n))
+    w[row, col] = vals
+    w[col, row] = vals
+    d = np.zeros(n)
+    if c.nrsq == 0:
+        d += min(1.0 / (r * r), 1.0e16) * c.cent
+    if c.nconst == 0:
+        d += c.eint
+    if c.conlen > 0.0:
+        d += r * r / c.conlen ** 4
+    return w + np.diag(d - ered)
+
+
+def adiabatic_wkb_y(c: Coupling, r: float, p: np.ndarray, ered: float, outward: bool,
+                    open_value: float = 0.0) -> np.ndarray:
+    """YINIT in the local eigenbasis of W(R) (yinit.f:96-117 with ADIAMN):
+    +-sqrt(lambda) for locally closed channels (+ outward, - inward), the
+    given value for locally open ones."""
+    lam, vec = np.linalg.eigh(w_matrix(c, r, p, ered))
+    sgn = 1.0 if outward else -1.0
+    yl = np.where(lam > 0.0, sgn * np.sqrt(np.abs(lam)), open_value)
+    return (vec * yl) @ vec.T
+
+
+@dataclass
+class BoundProblem:
+    """One (JTOT, block) system with its two propagation segments."""
+    coupling: Coupling
+    seg_out: Segment  # RMIN -> RMATCH
+    seg_in: Segment   # RMAX -> RMATCH (DR < 0)
+    prop: str = "LDMD"
+    y_out0: Callable[[float], np.ndarray] | None = None
+    y_in0: Callable[[float], np.ndarray] | None = None
+
+    def __post_init__(self):
+        c, so, si = self.coupling, self.seg_out, self.seg_in
+        if self.y_out0 is None:
+            self.y_out0 = lambda e: adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
+        if self.y_in0 is None:
+            self.y_in0 = lambda e: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
+
+
+def node_counts(bp: BoundProblem, ereds) -> tuple:
+    """(counts, NODES_out, NODES_in, matching counts, smallest matching
+    eigenvalue) at every ERED, the propagations of all energies in one plan."""
+    ereds = np.asarray(ereds, dtype=np.float64)
+    m = ereds.size
+    job_sys = np.concatenate([np.zeros(m, dtype=np.int32), np.ones(m, dtype=np.int32)])
+    job_e = np.concatenate([ereds, ereds])
+    plan = Plan(bp.prop, [bp.coupling, bp.coupling], [bp.seg_out, bp.seg_in], job_sys, job_e)
+    try:
+        y0 = [bp.y_out0(float(e)) for e in ereds] + [bp.y_in0(float(e)) for e in ereds]
+        ybuf, nodes, status, kfail = plan.run_host(plan.pack(y0))
+        if (status != 0).any():
+            j = int(np.nonzero(status)[0][0])
+            raise RuntimeError(f"propagation failed at ERED={job_e[j]} (status {int(status[j])}, step {int(kfail[j])})")
+        nmatch = np.zeros(m, dtype=np.int64)
+        eigmin = np.zeros(m)
+        for k in range(m):
+            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k))
+            nmatch[k] = int(np.sum(ev <= 0.0))
+            eigmin[k] = ev[np.argmin(np.abs(ev))]
+        n_out = nodes[:m].astype(np.int64)
+        n_in = nodes[m:].astype(np.int64)
+        return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
+    finally:
+        plan.close()
+
+
+def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_rounds: int = 200,
+                counter: Callable | None = None) -> list:
+    """Every state with EMIN < E < EMAX (reduced energies), bisected until its
+    bracket is narrower than tol.  Returns [(node count k, energy, lo, hi)]:
+    the state where the count steps from k to k+1 (the reference prints it as
+    state number k+1), at the bracket midpoint.  `counter(bp, ereds) ->
+    counts` defaults to the GPU node count."""
+    count = counter or (lambda b, e: node_counts(b, e)[0])
+    c0, c1 = (int(x) for x in count(bp, [emin, emax]))
+    brackets = {k: [emin, emax] for k in range(c0, c1)}
+    for _ in range(max_rounds):
+        live = [k for k, (lo, hi) in brackets.items() if hi - lo > tol]
+        if not live:
+            break
+        mids = np.array([0.5 * (brackets[k][0] + brackets[k][1]) for k in live])
+        counts = count(bp, mids)
+        for k, e, cnt in zip(live, mids, counts):
+            # tighten every bracket this energy informs
+            for kk, br in brackets.items():
+                if br[0] < e < br[1]:
+                    if cnt <= kk:
+                        br[0] = e
+                    else:
+                        br[1] = e
+    return [(k, 0.5 * (lo + hi), lo, hi) for k, (lo, hi) in sorted(brackets.items())]

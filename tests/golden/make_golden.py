@@ -1,8 +1,15 @@
-"""Extract golden S matrices from the reference's example outputs.
+"""Extract golden S matrices and bound-state energies from the reference's
+example outputs.
 
 Run in a checkout that has the reference project at $MOLSCAT_REF (default
-/root/reference); writes tests/golden/molscat_all_propagators.json.  The
-fixture is committed, so nothing at test time reads the reference tree.
+/root/reference); writes tests/golden/molscat_all_propagators.json and
+tests/golden/bound_basic1.json.  The fixtures are committed, so nothing at
+test time reads the reference tree.
+
+Bound states: examples/output/bound-basic1.output (the same model system,
+JTOT=1, symmetry block 2, MDPROP outward RMIN=0.5 -> RMATCH=1.0 and inward
+RMAX=20 -> RMATCH, DR=0.001, states between -10 and -1 cm-1), input
+examples/input/bound-basic1.input.
 
 Source: examples/output/molscat-all_propagators.output, runs
 "IPROPS=5" (LDPROP, lines 408-537) and "IPROPS=6" (MDPROP, lines 682-811):
@@ -16,6 +23,7 @@ import sys
 
 REF = os.environ.get("MOLSCAT_REF", "/root/reference")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "molscat_all_propagators.json")
+OUT_BOUND = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_basic1.json")
 
 
 def parse_runs(text):
@@ -66,5 +74,28 @@ def main():
     print("wrote", OUT, file=sys.stderr)
 
 
+def main_bound():
+    path = os.path.join(REF, "examples", "output", "bound-basic1.output")
+    with open(path) as f:
+        text = f.read()
+    states = [{"state": int(a), "energy_cm": float(b)} for a, b in
+              re.findall(r"CONVERGED ON STATE NUMBER\s+(\d+)\s+AT\s+ENERGY =\s+(\S+)\s+CM-1", text)]
+    doc = {
+        "source": "examples/output/bound-basic1.output (converged states), examples/input/bound-basic1.input",
+        "system": {
+            "itype": 1, "ured": 20.0, "be": 30.0, "jlevel": [0, 2, 4, 6],
+            "lambda": [0, 2], "terms": [[[1.0, -12, None], [-2.0, -6, None]], [[-0.2, -6, None]]],
+            "rm": 3.5, "epsil": 50.0, "jtot": 1, "block": 2,
+            "rmin": 0.5, "rmatch": 1.0, "rmax": 20.0, "dr": 0.001, "emin_cm": -10.0, "emax_cm": -1.0,
+            "convergence_cm": 1.0e-7,
+        },
+        "states": states,
+    }
+    with open(OUT_BOUND, "w") as f:
+        json.dump(doc, f, indent=1)
+    print("wrote", OUT_BOUND, file=sys.stderr)
+
+
 if __name__ == "__main__":
     main()
+    main_bound()

@@ -1,0 +1,90 @@
+"""Bound states by node counting against the reference's printed
+bound-basic1 energies (examples/output/bound-basic1.output: JTOT=1, block 2,
+states 4 and 5), with the propagations on the CPU oracle (pins the restated
+BOUND logic: segments, YINIT, node count, matching) and on the GPU (equal
+node counts at every energy, energies within 1e-9 relative of the oracle's)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from molscat_b200.bound import BoundProblem, adiabatic_wkb_y, find_states
+from molscat_b200.propagators import Coupling, Segment, radial_grid
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL_CM = 1.0e-9          # bisection width
+REF_TOL_CM = 2.0e-7      # the reference converged its steps to 1e-7 cm-1
+
+
+@pytest.fixture(scope="module")
+def basic1():
+    from oracle import oracle as O
+    with open(os.path.join(HERE, "golden", "bound_basic1.json")) as f:
+        g = json.load(f)
+    s = g["system"]
+    sysm = O.Itype1(ured=s["ured"], be=s["be"], jlevel=s["jlevel"], lam=s["lambda"],
+                    terms=[[tuple(t) for t in tl] for tl in s["terms"]], rm=s["rm"], epsil=s["epsil"])
+    oc = sysm.coupling(s["jtot"], s["block"])
+    c = Coupling(n=oc.n, nham=oc.nham, vl=oc.vl, eint=oc.eint, cent=oc.cent)
+    n_out = int(round((s["rmatch"] - s["rmin"]) / s["dr"]))
+    n_in = int(round((s["rmax"] - s["rmatch"]) / s["dr"]))
+    r_out = radial_grid(s["rmin"], (s["rmatch"] - s["rmin"]) / n_out, n_out)
+    r_in = radial_grid(s["rmax"], -(s["rmax"] - s["rmatch"]) / n_in, n_in)
+    seg_out = Segment(n_out, (s["rmatch"] - s["rmin"]) / n_out, r_out, O.ptable(sysm, r_out))
+    seg_in = Segment(n_in, -(s["rmax"] - s["rmatch"]) / n_in, r_in, O.ptable(sysm, r_in))
+    return g, sysm, BoundProblem(c, seg_out, seg_in, "LDMD")
+
+
+def oracle_counts(bp, ereds):
+    from oracle import oracle as O
+    oc = cases.to_oracle(bp.coupling)
+    out = []
+    for e in ereds:
+        yo, no, st, _ = O.mdprop(oc, bp.seg_out.rtab, bp.seg_out.ptab, bp.seg_out.nstep, bp.seg_out.dr, e,
+                                 bp.y_out0(float(e)))
+        yi, ni, st2, _ = O.mdprop(oc, bp.seg_in.rtab, bp.seg_in.ptab, bp.seg_in.nstep, bp.seg_in.dr, e,
+                                  bp.y_in0(float(e)))
+        assert st == 0 and st2 == 0
+        out.append(no + ni + int(np.sum(np.linalg.eigvalsh(yo - yi) <= 0.0)))
+    return np.array(out)
+
+
+def _states(bp, sysm, g, counter=None):
+    """(the reference's 1-based state number, energy in cm-1): the state where
+    the count steps from k to k+1 is state k+1."""
+    s = g["system"]
+    res = find_states(bp, s["emin_cm"] * sysm.cm2ru, s["emax_cm"] * sysm.cm2ru, TOL_CM * sysm.cm2ru,
+                      counter=counter)
+    return [(k + 1, e / sysm.cm2ru) for k, e, _, _ in res]
+
+
+def test_oracle_reproduces_reference_bound_states(basic1):
+    g, sysm, bp = basic1
+    got = _states(bp, sysm, g, counter=oracle_counts)
+    want = [(st["state"], st["energy_cm"]) for st in g["states"]]
+    assert [k for k, _ in got] == [k for k, _ in want]
+    for (_, e), (_, w) in zip(got, want):
+        assert abs(e - w) < REF_TOL_CM, (e, w)
+
+
+@pytest.mark.gpu
+def test_gpu_bound_states_equal_oracle(basic1):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from molscat_b200.bound import node_counts
+    g, sysm, bp = basic1
+    got = _states(bp, sysm, g)
+    want = [(st["state"], st["energy_cm"]) for st in g["states"]]
+    assert [k for k, _ in got] == [k for k, _ in want]
+    for (_, e), (_, w) in zip(got, want):
+        assert abs(e - w) < REF_TOL_CM, (e, w)
+    # node counts identical to the oracle's, also right beside each state
+    probe = [-9.0, -6.0, -3.0] + [e + d for _, e in got for d in (-1e-6, 1e-6)]
+    ered = np.array(probe) * sysm.cm2ru
+    assert np.array_equal(node_counts(bp, ered)[0], oracle_counts(bp, ered))
+    ora = _states(bp, sysm, g, counter=oracle_counts)
+    for (_, e), (_, o) in zip(got, ora):
+        assert abs(e - o) <= 1e-9 * abs(o) + 2 * TOL_CM

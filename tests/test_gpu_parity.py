@@ -230,3 +230,17 @@ def test_batched_large_n_family_at_small_n(prop, n):
     yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
     assert st == 0 and ng == no
     assert cases.rel_err(yg, yo) < Y_TOL
+
+
+@pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
+@pytest.mark.parametrize("n", [100, 260])
+@pytest.mark.parametrize("kw", [dict(ivlfl=1), dict(nconst=1, nrsq=1, conlen=3.0), dict(inward=True)],
+                         ids=["iv", "const-rsq-conf", "inward"])
+def test_hammat_variants_large(prop, n, kw):
+    """IV indexing, NCONST/NRSQ/CONLEN and inward propagation through the
+    one-CTA (N = 100) and batched large-N (N = 260) kernels."""
+    c, seg, ered, y0 = cases.random_case(n, 40, seed=88 + n, **kw)
+    yg, ng = propagate(prop, c, seg, ered, y0)
+    yo, no, st, _ = oracle_prop(prop, c, seg, ered, y0)
+    assert st == 0 and ng == no
+    assert cases.rel_err(yg, yo) < Y_TOL
