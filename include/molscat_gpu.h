@@ -113,7 +113,10 @@ int mgpu_plan_run_host(mgpu_plan *plan, double *y, int *nodes, int *status, int 
 
 /* Device buffers (y_dev in/out, nodes_dev/status_dev/kfail_dev out) on the
  * given cudaStream_t passed as void* (NULL = legacy default stream).
- * Asynchronous: returns after the launches are queued. */
+ * Asynchronous: returns after the launches are queued.  Each large-N bucket
+ * runs on a stream pair of the plan's own, forked from and joined back into
+ * `stream`, so buckets of different N overlap; the stream must therefore not
+ * be capturing a graph. */
 int mgpu_plan_run_device(mgpu_plan *plan, double *y_dev, int *nodes_dev,
                          int *status_dev, int *kfail_dev, void *stream);
 

@@ -957,9 +957,16 @@ struct mgpu_plan {
     int *d_nb = nullptr, *d_nb_off = nullptr;
     double *d_sr = nullptr, *d_si = nullptr;
     size_t s_cap = 0;
-    cudaStream_t side = nullptr;           // look-ahead stream of the large-N inversions
-    cudaStream_t own = nullptr;            // the large-N work (never the legacy stream: graph capture)
-    cudaEvent_t evf = nullptr, evj = nullptr, ev_in = nullptr, ev_out = nullptr;
+    // Streams of the large-N buckets: each bucket's step loop runs on its own
+    // stream (never the legacy stream: graph capture) with a high-priority
+    // look-ahead stream beside it, so buckets of different N overlap on the GPU.
+    struct BigStreams {
+        cudaStream_t st = nullptr, side = nullptr;
+        cudaEvent_t evf = nullptr, evj = nullptr, done = nullptr;
+    };
+    std::vector<BigStreams> bstreams;
+    cudaStream_t own = nullptr;            // run_host's copies and launches
+    cudaEvent_t ev_in = nullptr;
     // host staging for run_host
     double *d_y = nullptr;
     int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
@@ -969,13 +976,18 @@ struct mgpu_plan {
     ~mgpu_plan()
     {
         if (own) cudaStreamSynchronize(own);
+        for (auto &q : bstreams)
+            if (q.st) cudaStreamSynchronize(q.st);
         for (auto &g : big)
             if (g.step_graph) cudaGraphExecDestroy(g.step_graph);
-        if (evf) cudaEventDestroy(evf);
-        if (evj) cudaEventDestroy(evj);
+        for (auto &q : bstreams) {
+            if (q.evf) cudaEventDestroy(q.evf);
+            if (q.evj) cudaEventDestroy(q.evj);
+            if (q.done) cudaEventDestroy(q.done);
+            if (q.side) cudaStreamDestroy(q.side);
+            if (q.st) cudaStreamDestroy(q.st);
+        }
         if (ev_in) cudaEventDestroy(ev_in);
-        if (ev_out) cudaEventDestroy(ev_out);
-        if (side) cudaStreamDestroy(side);
         if (own) cudaStreamDestroy(own);
         for (void *p : allocs) cudaFree(p);
         if (d_y) cudaFree(d_y);
@@ -1522,15 +1534,18 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     for (size_t slot = 0; slot < p->bucket_ids.size(); ++slot) {
         const int b = p->bucket_ids[slot];
         if (kBuckets[b].kind != KIND_BIG) continue;
-        if (p->big.empty()) {
+        {
             int lo = 0, hi = 0;
+            p->bstreams.emplace_back();
+            mgpu_plan::BigStreams &q = p->bstreams.back();
             if ((e = cudaDeviceGetStreamPriorityRange(&lo, &hi)) ||
-                (e = cudaStreamCreateWithPriority(&p->side, cudaStreamNonBlocking, hi)) ||
-                (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)) ||
-                (e = cudaEventCreateWithFlags(&p->evf, cudaEventDisableTiming)) ||
-                (e = cudaEventCreateWithFlags(&p->evj, cudaEventDisableTiming)) ||
-                (e = cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming)) ||
-                (e = cudaEventCreateWithFlags(&p->ev_out, cudaEventDisableTiming)) || (e = big_kernel_attributes())) {
+                (e = cudaStreamCreateWithPriority(&q.side, cudaStreamNonBlocking, hi)) ||
+                (e = cudaStreamCreateWithFlags(&q.st, cudaStreamNonBlocking)) ||
+                (e = cudaEventCreateWithFlags(&q.evf, cudaEventDisableTiming)) ||
+                (e = cudaEventCreateWithFlags(&q.evj, cudaEventDisableTiming)) ||
+                (e = cudaEventCreateWithFlags(&q.done, cudaEventDisableTiming)) ||
+                (!p->ev_in && (e = cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming))) ||
+                (e = big_kernel_attributes())) {
                 delete p;
                 return set_err(MGPU_ERR_CUDA, "large-N set-up", e);
             }
@@ -1628,26 +1643,32 @@ int mgpu_plan_run_device_phases(mgpu_plan *p, double *y_dev, int *nodes_dev, int
         }
     }
     if (!p->big.empty()) {
-        // the large-N work runs on the plan's own stream, ordered after and before the caller's
-        if ((e = cudaEventRecord(p->ev_in, st)) || (e = cudaStreamWaitEvent(p->own, p->ev_in, 0)))
-            return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
-        if (p->iprop == MGPU_PROP_LDMD && (phases & 1))
-            for (const auto &g : p->big)
-                if ((e = run_big_prep(g, p->d_sys, p->sys_nstep, p->own, p->side, p->evf, p->evj)))
-                    return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
-        for (auto &g : p->big)
+        // every large-N bucket on its own stream pair, ordered after the caller's stream
+        if ((e = cudaEventRecord(p->ev_in, st))) return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
+        for (size_t i = 0; i < p->big.size(); ++i) {
+            BigBucket &g = p->big[i];
+            const mgpu_plan::BigStreams &q = p->bstreams[i];
+            if ((e = cudaStreamWaitEvent(q.st, p->ev_in, 0))) return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
+            if (p->iprop == MGPU_PROP_LDMD && (phases & 1) &&
+                (e = run_big_prep(g, p->d_sys, p->sys_nstep, q.st, q.side, q.evf, q.evj)))
+                return set_err(MGPU_ERR_CUDA, "large-N preparation", e);
             if ((phases & 2) && (e = run_big_prop(g, p->iprop, p->d_sys, y_dev, nodes_dev, status_dev, kfail_dev,
-                                                  p->own, p->side, p->evf, p->evj)))
+                                                  q.st, q.side, q.evf, q.evj)))
                 return set_err(MGPU_ERR_CUDA, "large-N propagation", e);
-        if ((e = cudaEventRecord(p->ev_out, p->own)) || (e = cudaStreamWaitEvent(st, p->ev_out, 0)))
-            return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
+            if ((e = cudaEventRecord(q.done, q.st))) return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
+        }
     }
+    // the small-N buckets on the caller's stream, beside the large-N streams
     for (size_t b = 0; b < p->bucket_ids.size() && (phases & 2); ++b) {
         if (p->job_count[b] == 0 || kBuckets[p->bucket_ids[b]].kind == KIND_BIG) continue;
         if ((e = launch_prop(p->iprop, p->bucket_ids[b], p->job_count[b], p->smem[b], p->vl_smem[b], st, p->d_sys,
                              p->d_jobs + p->job_begin[b], y_dev, nodes_dev, status_dev, kfail_dev)))
             return set_err(MGPU_ERR_CUDA, "launching the propagation kernel", e);
     }
+    // the caller's stream waits for every large-N bucket
+    for (size_t i = 0; i < p->big.size(); ++i)
+        if ((e = cudaStreamWaitEvent(st, p->bstreams[i].done, 0)))
+            return set_err(MGPU_ERR_CUDA, "ordering the large-N work", e);
     return MGPU_OK;
 }
 
