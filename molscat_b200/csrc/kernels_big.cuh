@@ -37,7 +37,16 @@ constexpr int KB = NB / 8;  // tile columns per round
 constexpr int MC = NB / 4;  // m8n8k4 k-steps per round
 constexpr int FACT_THREADS = 512;
 constexpr int PANEL_WARPS = 8;
-constexpr int UPD_WARPS = 4;
+#ifndef MGPU_UPD_WARPS
+#define MGPU_UPD_WARPS 4
+#endif
+constexpr int UPD_WARPS = MGPU_UPD_WARPS;  // warps of an update CTA (64x64 block of C)
+constexpr int UPD_RPW = 8 / UPD_WARPS;     // tile rows per warp
+static_assert(UPD_WARPS * UPD_RPW == 8, "an update CTA covers 8 tile rows");
+#ifndef MGPU_UPD_UNROLL
+#define MGPU_UPD_UNROLL 2
+#endif
+constexpr int UPD_UNROLL = MGPU_UPD_UNROLL;  // k-steps of the update loop unrolled
 constexpr int EW_THREADS = 256;
 constexpr int kBigMaxNT = 128;  // NPAD <= 1024
 
@@ -372,10 +381,10 @@ big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round,
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool inP = (BI == round) || (BJ == round);  // whole tiles of row/column block P
-    const int I0 = 8 * BI + 2 * warp;
-    double acc[2][KB][2];
+    const int I0 = 8 * BI + UPD_RPW * warp;
+    double acc[UPD_RPW][KB][2];
 #pragma unroll
-    for (int ii = 0; ii < 2; ++ii)
+    for (int ii = 0; ii < UPD_RPW; ++ii)
 #pragma unroll
         for (int jt = 0; jt < KB; ++jt) {
             const int I = I0 + ii, J = 8 * BJ + jt;
@@ -389,20 +398,23 @@ big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round,
         mbar_wait_bounded(&bar, 0);  // let the copies land before the CTA's shared memory goes
         return;
     }
-    const double *xa = Xs + (2 * warp) * MC * 32 + lane;
-#pragma unroll 2
+    const double *xa = Xs + (UPD_RPW * warp) * MC * 32 + lane;
+#pragma unroll UPD_UNROLL
     for (int mc = 0; mc < MC; ++mc) {
-        const double a0 = xa[mc * 32], a1 = xa[MC * 32 + mc * 32];
+        double a[UPD_RPW];
+#pragma unroll
+        for (int ii = 0; ii < UPD_RPW; ++ii) a[ii] = xa[ii * MC * 32 + mc * 32];
 #pragma unroll
         for (int jt = 0; jt < KB; ++jt) {
             const double b = Bs[(jt * MC + mc) * 32 + lane];
             const int J = 8 * BJ + jt;
-            if (I0 >= J) wf::dmma(acc[0][jt][0], acc[0][jt][1], a0, b);
-            if (I0 + 1 >= J) wf::dmma(acc[1][jt][0], acc[1][jt][1], a1, b);
+#pragma unroll
+            for (int ii = 0; ii < UPD_RPW; ++ii)
+                if (I0 + ii >= J) wf::dmma(acc[ii][jt][0], acc[ii][jt][1], a[ii], b);
         }
     }
 #pragma unroll
-    for (int ii = 0; ii < 2; ++ii)
+    for (int ii = 0; ii < UPD_RPW; ++ii)
 #pragma unroll
         for (int jt = 0; jt < KB; ++jt) {
             const int I = I0 + ii, J = 8 * BJ + jt;
