@@ -40,9 +40,14 @@ constexpr int PANEL_WARPS = 8;
 #ifndef MGPU_UPD_WARPS
 #define MGPU_UPD_WARPS 4
 #endif
-constexpr int UPD_WARPS = MGPU_UPD_WARPS;  // warps of an update CTA (64x64 block of C)
-constexpr int UPD_RPW = 8 / UPD_WARPS;     // tile rows per warp
-static_assert(UPD_WARPS * UPD_RPW == 8, "an update CTA covers 8 tile rows");
+#ifndef MGPU_UPD_ROWS
+#define MGPU_UPD_ROWS 4
+#endif
+constexpr int UPD_WARPS = MGPU_UPD_WARPS;     // warps of an update CTA
+constexpr int UPD_ROWS = MGPU_UPD_ROWS;       // tile rows of C per CTA (8: a whole 64x64 block)
+constexpr int UPD_SPLIT = 8 / UPD_ROWS;       // CTAs per 64x64 block
+constexpr int UPD_RPW = UPD_ROWS / UPD_WARPS; // tile rows per warp
+static_assert(UPD_WARPS * UPD_RPW == UPD_ROWS && UPD_SPLIT * UPD_ROWS == 8, "update CTA shape");
 #ifndef MGPU_UPD_UNROLL
 #define MGPU_UPD_UNROLL 2
 #endif
@@ -345,10 +350,12 @@ big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, 
 // update: A_IJ = [IJ outside P] A_IJ + X_I B_J^T over a block of 8x8 tiles
 // ---------------------------------------------------------------------------
 constexpr uint32_t kUpdHalfBytes = KB * MC * 32 * sizeof(double);  // 32 KB: 8 tile rows of X (or B)
-constexpr size_t kUpdSmem = 2 * (size_t)kUpdHalfBytes;
+constexpr uint32_t kUpdXBytes = kUpdHalfBytes / UPD_SPLIT;         // X rows of one CTA
+constexpr size_t kUpdSmem = (size_t)kUpdHalfBytes + kUpdXBytes;
 
 // Which 64x64 blocks of tiles a launch updates: all of them, only block row and
-// column `cblk` (grid.x = NT/8), or all but those (the look-ahead split).
+// column `cblk` (grid.x = UPD_SPLIT * NT/8), or all but those (the look-ahead
+// split).  UPD_SPLIT consecutive CTAs share one block, UPD_ROWS tile rows each.
 enum { UPD_ALL = 0, UPD_ONLY = 1, UPD_EXCEPT = 2 };
 
 __global__ void __launch_bounds__(32 * UPD_WARPS)
@@ -361,27 +368,28 @@ big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round,
     const MatDesc md = mds[m];
     if (*kstep > md.nstep) return;
     int BI, BJ;
+    const int blk = (int)blockIdx.x / UPD_SPLIT, part = (int)blockIdx.x % UPD_SPLIT;
     if (mode == UPD_ONLY) {
-        const int x = blockIdx.x;
+        const int x = blk;
         BI = x <= cblk ? cblk : x;
         BJ = x <= cblk ? x : cblk;
     } else {
-        tile_ij(blockIdx.x, BI, BJ);
+        tile_ij(blk, BI, BJ);
         if (mode == UPD_EXCEPT && (BI == cblk || BJ == cblk)) return;  // whole CTA
     }
-    double *Xs = usm, *Bs = usm + KB * MC * 32;
+    double *Xs = usm, *Bs = usm + kUpdXBytes / sizeof(double);
     if (threadIdx.x == 0) {
         mbar_init(&bar, 2);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        bulk_load(Xs, pn.xf + ((size_t)m * nt + 8 * BI) * MC * 32, kUpdHalfBytes, &bar);
+        bulk_load(Xs, pn.xf + ((size_t)m * nt + 8 * BI + UPD_ROWS * part) * MC * 32, kUpdXBytes, &bar);
         bulk_load(Bs, pn.bf + ((size_t)m * nt + 8 * BJ) * MC * 32, kUpdHalfBytes, &bar);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool inP = (BI == round) || (BJ == round);  // whole tiles of row/column block P
-    const int I0 = 8 * BI + UPD_RPW * warp;
+    const int I0 = 8 * BI + UPD_ROWS * part + UPD_RPW * warp;
     double acc[UPD_RPW][KB][2];
 #pragma unroll
     for (int ii = 0; ii < UPD_RPW; ++ii)

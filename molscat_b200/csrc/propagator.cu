@@ -683,7 +683,7 @@ static int bucket_for(int n, int iprop = MGPU_PROP_LDMD, bool tuned = true)
 template <class K>
 static cudaError_t set_smem(K kernel, size_t bytes)
 {
-    if (bytes <= 48 * 1024) return cudaSuccess;
+    if (bytes == 0) return cudaSuccess;
     static std::mutex mu;
     static std::vector<std::pair<std::pair<int, const void *>, size_t>> done;
     int dev = 0;
@@ -692,12 +692,19 @@ static cudaError_t set_smem(K kernel, size_t bytes)
     std::lock_guard<std::mutex> lk(mu);
     for (auto &d : done)
         if (d.first.first == dev && d.first.second == key && d.second >= bytes) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    // the 48 KB default covers static plus dynamic shared memory
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, (const void *)kernel);
     if (e != cudaSuccess) return e;
-    // resident CTAs are limited by registers, not by the L1/shared split
-    e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-    if (e == cudaSuccess) done.push_back({{dev, key}, bytes});
-    return e;
+    if (bytes + fa.sharedSizeBytes > 48 * 1024) {
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        if (e != cudaSuccess) return e;
+        // resident CTAs are limited by registers, not by the L1/shared split
+        e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
+    done.push_back({{dev, key}, bytes});
+    return cudaSuccess;
 }
 
 // grid.x counts steps, grid.y systems
@@ -1027,7 +1034,8 @@ static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::
 {
     const int rounds = nt / big::KB;
     const int nbk = nt / 8;
-    const dim3 gp((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), gall(nbk * (nbk + 1) / 2, M), gcol(nbk, M);
+    const dim3 gp((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), gall(big::UPD_SPLIT * nbk * (nbk + 1) / 2, M),
+        gcol(big::UPD_SPLIT * nbk, M);
     const int ut = 32 * big::UPD_WARPS, pt = 32 * big::PANEL_WARPS;
     cudaError_t e;
     big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn[0], 0, kstep);
