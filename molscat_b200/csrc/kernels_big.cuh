@@ -353,10 +353,12 @@ constexpr uint32_t kUpdHalfBytes = KB * MC * 32 * sizeof(double);  // 32 KB: 8 t
 constexpr uint32_t kUpdXBytes = kUpdHalfBytes / UPD_SPLIT;         // X rows of one CTA
 constexpr size_t kUpdSmem = (size_t)kUpdHalfBytes + kUpdXBytes;
 
-// Which 64x64 blocks of tiles a launch updates: all of them, only block row and
-// column `cblk` (grid.x = UPD_SPLIT * NT/8), or all but those (the look-ahead
-// split).  UPD_SPLIT consecutive CTAs share one block, UPD_ROWS tile rows each.
-enum { UPD_ALL = 0, UPD_ONLY = 1, UPD_EXCEPT = 2 };
+// Which 64x64 blocks of tiles a launch updates: all of them; only block row and
+// column `cblk` without the diagonal block (grid.x = UPD_SPLIT * (NT/8 - 1));
+// all but block row and column `cblk`; only the diagonal block (cblk, cblk)
+// (grid.x = UPD_SPLIT) -- the look-ahead split.  UPD_SPLIT consecutive CTAs
+// share one block, UPD_ROWS tile rows each.
+enum { UPD_ALL = 0, UPD_ONLY = 1, UPD_EXCEPT = 2, UPD_DIAG = 3 };
 
 __global__ void __launch_bounds__(32 * UPD_WARPS)
 big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep,
@@ -369,10 +371,12 @@ big_update_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round,
     if (*kstep > md.nstep) return;
     int BI, BJ;
     const int blk = (int)blockIdx.x / UPD_SPLIT, part = (int)blockIdx.x % UPD_SPLIT;
-    if (mode == UPD_ONLY) {
-        const int x = blk;
-        BI = x <= cblk ? cblk : x;
-        BJ = x <= cblk ? x : cblk;
+    if (mode == UPD_DIAG) {
+        BI = BJ = cblk;
+    } else if (mode == UPD_ONLY) {
+        const int x = blk < cblk ? blk : blk + 1;  // block row cblk left of the diagonal, column cblk below it
+        BI = x < cblk ? cblk : x;
+        BJ = x < cblk ? x : cblk;
     } else {
         tile_ij(blk, BI, BJ);
         if (mode == UPD_EXCEPT && (BI == cblk || BJ == cblk)) return;  // whole CTA

@@ -1025,17 +1025,19 @@ static cudaError_t upload(mgpu_plan *p, X **dst, const X *src, size_t count)
 }
 
 // -A^{-1} in place for M matrices of a large-N bucket, 64 pivots a round
-// (factor, panel and update kernels).  Look-ahead: once the tile row and
-// column that form the next round's panel are updated, the next round's
-// factor and panel run on the high-priority `side` stream while `st` updates
-// the remaining tiles; the X/B operands alternate between two buffers.
+// (factor, panel and update kernels).  Look-ahead: once the next round's
+// diagonal block is updated, its factor runs on the high-priority `side`
+// stream; once the rest of the next panel's tile row and column is updated,
+// the next round's panel follows it there, while `st` updates the remaining
+// tiles; the X/B operands alternate between two buffers.  `evf` is recorded
+// twice a round: each wait on it takes the record made just before.
 static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::Panels (&pn)[2], const int *kstep,
                               cudaStream_t st, cudaStream_t side, cudaEvent_t evf, cudaEvent_t evj)
 {
     const int rounds = nt / big::KB;
     const int nbk = nt / 8;
     const dim3 gp((nt + big::PANEL_WARPS - 1) / big::PANEL_WARPS, M), gall(big::UPD_SPLIT * nbk * (nbk + 1) / 2, M),
-        gcol(big::UPD_SPLIT * nbk, M);
+        gcol(big::UPD_SPLIT * (nbk - 1), M), gdiag(big::UPD_SPLIT, M);
     const int ut = 32 * big::UPD_WARPS, pt = 32 * big::PANEL_WARPS;
     cudaError_t e;
     big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn[0], 0, kstep);
@@ -1043,9 +1045,11 @@ static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::
     for (int R = 0; R < rounds; ++R) {
         const big::Panels &cur = pn[R & 1], &nxt = pn[(R + 1) & 1];
         if (R + 1 < rounds) {
-            big::big_update_kernel<<<gcol, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_ONLY, R + 1);
+            big::big_update_kernel<<<gdiag, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_DIAG, R + 1);
             if ((e = cudaEventRecord(evf, st)) || (e = cudaStreamWaitEvent(side, evf, 0))) return e;
             big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, side>>>(md, nxt, R + 1, kstep);
+            big::big_update_kernel<<<gcol, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_ONLY, R + 1);
+            if ((e = cudaEventRecord(evf, st)) || (e = cudaStreamWaitEvent(side, evf, 0))) return e;
             big::big_panel_kernel<<<gp, pt, 0, side>>>(md, nxt, nt, R + 1, kstep);
             if ((e = cudaEventRecord(evj, side))) return e;
             big::big_update_kernel<<<gall, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_EXCEPT, R + 1);
@@ -1232,7 +1236,7 @@ static cudaError_t run_big_prep(const BigBucket &g, const SysDev *d_sys, const s
 
 // The step loop of a large-N bucket: start, NSTEP x (elementwise, inversions),
 // results into y / nodes / status / kfail (indexed by JobDev::yoff / ::out).
-// `st` must not be the legacy default stream: one step (its ~4 x NT/8 x 2
+// `st` must not be the legacy default stream: one step (its ~5 x NT/8 x 2
 // launches, look-ahead fork/join included) is captured into a CUDA graph on
 // first use and replayed NSTEP times; the device-side step counter makes
 // every replay the next step.  The graph stays in g.step_graph for reuse.
@@ -1404,7 +1408,8 @@ int mgpu_plan_launches(const mgpu_plan *p)
         if (p->job_count[b] > 0) ++l;
     }
     for (const auto &g : p->big) {
-        const int per_inv = 4 * (g.nt / big::KB) - 1;  // factor, panel, two update launches; one update in the last round
+        // first factor and panel; then a round: three update launches, factor, panel; one update in the last round
+        const int per_inv = 5 * (g.nt / big::KB) - 2;
         if (p->iprop == MGPU_PROP_LDMD)
             for (size_t i = 0; i < g.prep_sys.size(); ++i) {
                 const int ns = p->sys_nstep[g.prep_sys[i]];
