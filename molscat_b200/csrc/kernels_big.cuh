@@ -35,7 +35,11 @@ using wf::tix;
 constexpr int NB = 64;      // pivots per round
 constexpr int KB = NB / 8;  // tile columns per round
 constexpr int MC = NB / 4;  // m8n8k4 k-steps per round
+// Factor CTA sizes: a whole SM's registers (1024 threads at 64) where the
+// update beside it is small (NT <= FACT_BIG_MAX_NT), half of them above.
 constexpr int FACT_THREADS = 512;
+constexpr int FACT_THREADS_BIG = 1024;
+constexpr int FACT_BIG_MAX_NT = 32;
 constexpr int PANEL_WARPS = 8;
 #ifndef MGPU_UPD_WARPS
 #define MGPU_UPD_WARPS 4
@@ -120,9 +124,14 @@ __device__ __forceinline__ void report_failure(const MatDesc &md, int flags, int
 // rank-4 updates.
 // ---------------------------------------------------------------------------
 constexpr size_t kFactSmem = 2 * (size_t)NB * (NB + 1) * sizeof(double);  // D and Lam, padded rows
-constexpr int kFactOwn = FACT_THREADS - 32;                                // threads owning elements
-constexpr int kFactD = (NB * (NB + 1) / 2 + kFactOwn - 1) / kFactOwn;      // D elements per thread
-constexpr int kFactL = (NB * (NB - 1) / 2 + kFactOwn - 1) / kFactOwn;      // Lam elements per thread
+// element ownership in a factor CTA of T threads (warp 0 factors the sub-blocks)
+template <int T>
+struct FactShape {
+    static_assert(T >= 5 * NB && T % 32 == 0, "factor CTA: 4 NB rows of c(i) and every Lam column at once");
+    static constexpr int own = T - 32;                                   // threads owning elements
+    static constexpr int d = (NB * (NB + 1) / 2 + own - 1) / own;        // D elements per thread
+    static constexpr int l = (NB * (NB - 1) / 2 + own - 1) / own;        // Lam elements per thread
+};
 
 __device__ __forceinline__ void tri_rc(int e, int &i, int &j)  // e -> (i, j), j <= i
 {
@@ -133,9 +142,11 @@ __device__ __forceinline__ void tri_rc(int e, int &i, int &j)  // e -> (i, j), j
     j = e - r * (r + 1) / 2;
 }
 
-__global__ void __launch_bounds__(FACT_THREADS)
+template <int T>
+__global__ void __launch_bounds__(T)
 big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const int *__restrict__ kstep)
 {
+    constexpr int kFactOwn = FactShape<T>::own, kFactD = FactShape<T>::d, kFactL = FactShape<T>::l;
     extern __shared__ __align__(16) double fsm[];
     double (*D)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm);
     double (*L)[NB + 1] = reinterpret_cast<double (*)[NB + 1]>(fsm + NB * (NB + 1));
@@ -150,7 +161,7 @@ big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const i
     const int p0 = NB * round, K0 = KB * round;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (tid == 0) s_cnt = s_flags = 0;
-    for (int x = tid; x < NB * NB; x += FACT_THREADS) {
+    for (int x = tid; x < NB * NB; x += T) {
         const int i = x >> 6, j = x & 63;
         double v = 0.0;
         if (j <= i) v = md.a[(size_t)tix(K0 + (i >> 3), K0 + (j >> 3)) * 64 + ((i & 7) * 4 + ((j & 7) >> 1)) * 2 + (j & 1)];
@@ -279,7 +290,7 @@ big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const i
     }
     __syncthreads();
     double *lam = pn.lam + (size_t)blockIdx.x * NB * NB;
-    for (int x = tid; x < NB * NB; x += FACT_THREADS) lam[x] = L[x >> 6][x & 63];
+    for (int x = tid; x < NB * NB; x += T) lam[x] = L[x >> 6][x & 63];
     if (tid < NB) pn.rd[(size_t)blockIdx.x * NB + tid] = s_r[tid];
     if (tid == 0) {
         if (s_cnt) atomicAdd(md.cnt, md.sign * s_cnt);

@@ -1040,14 +1040,20 @@ static cudaError_t big_invert(const big::MatDesc *md, int M, int nt, const big::
         gcol(big::UPD_SPLIT * (nbk - 1), M), gdiag(big::UPD_SPLIT, M);
     const int ut = 32 * big::UPD_WARPS, pt = 32 * big::PANEL_WARPS;
     cudaError_t e;
-    big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, st>>>(md, pn[0], 0, kstep);
+    auto factor = [&](const big::Panels &p, int R, cudaStream_t s) {
+        if (nt <= big::FACT_BIG_MAX_NT)
+            big::big_factor_kernel<big::FACT_THREADS_BIG><<<M, big::FACT_THREADS_BIG, big::kFactSmem, s>>>(md, p, R, kstep);
+        else
+            big::big_factor_kernel<big::FACT_THREADS><<<M, big::FACT_THREADS, big::kFactSmem, s>>>(md, p, R, kstep);
+    };
+    factor(pn[0], 0, st);
     big::big_panel_kernel<<<gp, pt, 0, st>>>(md, pn[0], nt, 0, kstep);
     for (int R = 0; R < rounds; ++R) {
         const big::Panels &cur = pn[R & 1], &nxt = pn[(R + 1) & 1];
         if (R + 1 < rounds) {
             big::big_update_kernel<<<gdiag, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_DIAG, R + 1);
             if ((e = cudaEventRecord(evf, st)) || (e = cudaStreamWaitEvent(side, evf, 0))) return e;
-            big::big_factor_kernel<<<M, big::FACT_THREADS, big::kFactSmem, side>>>(md, nxt, R + 1, kstep);
+            factor(nxt, R + 1, side);
             big::big_update_kernel<<<gcol, ut, big::kUpdSmem, st>>>(md, cur, nt, R, kstep, big::UPD_ONLY, R + 1);
             if ((e = cudaEventRecord(evf, st)) || (e = cudaStreamWaitEvent(side, evf, 0))) return e;
             big::big_panel_kernel<<<gp, pt, 0, side>>>(md, nxt, nt, R + 1, kstep);
@@ -1295,7 +1301,8 @@ static cudaError_t run_big_prop(BigBucket &g, int iprop, const SysDev *d_sys, do
 static cudaError_t big_kernel_attributes()
 {
     cudaError_t e;
-    if ((e = set_smem(big::big_update_kernel, big::kUpdSmem)) || (e = set_smem(big::big_factor_kernel, big::kFactSmem)))
+    if ((e = set_smem(big::big_update_kernel, big::kUpdSmem)) || (e = set_smem(big::big_factor_kernel<big::FACT_THREADS>, big::kFactSmem)) ||
+        (e = set_smem(big::big_factor_kernel<big::FACT_THREADS_BIG>, big::kFactSmem)))
         return e;
     return cudaSuccess;
 }
