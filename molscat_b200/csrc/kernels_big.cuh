@@ -289,8 +289,12 @@ big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const i
         }
     }
     __syncthreads();
+    // Lam in the panel's B-fragment order: (row 8kt + ln/4, column 4mc + ln%4) at (kt MC + mc) 32 + ln
     double *lam = pn.lam + (size_t)blockIdx.x * NB * NB;
-    for (int x = tid; x < NB * NB; x += T) lam[x] = L[x >> 6][x & 63];
+    for (int x = tid; x < NB * NB; x += T) {
+        const int ln = x & 31, mc = (x >> 5) % MC, kt = x / (32 * MC);
+        lam[x] = L[8 * kt + (ln >> 2)][4 * mc + (ln & 3)];
+    }
     if (tid < NB) pn.rd[(size_t)blockIdx.x * NB + tid] = s_r[tid];
     if (tid == 0) {
         if (s_cnt) atomicAdd(md.cnt, md.sign * s_cnt);
@@ -304,31 +308,43 @@ big_factor_kernel(const MatDesc *__restrict__ mds, Panels pn, int round, const i
 __global__ void __launch_bounds__(32 * PANEL_WARPS)
 big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, const int *__restrict__ kstep)
 {
-    __shared__ __align__(16) double lamB[KB][MC][32];
+    // B fragments of Lam^T, as the factor wrote them: (k-row q, column r) of output tile kt, k-step mc
+    __shared__ __align__(128) double lamB[KB][MC][32];
     __shared__ double s_r[NB];
+    __shared__ __align__(8) uint64_t bar;
     const int m = blockIdx.y;
     const MatDesc md = mds[m];
     if (*kstep > md.nstep) return;
-    const double *lam = pn.lam + (size_t)m * NB * NB;
-    // B fragments of Lam^T: (k-row q, column r) of output tile kt, k-step mc
-    for (int x = threadIdx.x; x < KB * MC * 32; x += blockDim.x) {
-        const int ln = x & 31, mc = (x >> 5) % MC, kt = x / (32 * MC);
-        lamB[kt][mc][ln] = lam[(8 * kt + (ln >> 2)) * NB + 4 * mc + (ln & 3)];
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (threadIdx.x < NB) s_r[threadIdx.x] = pn.rd[(size_t)m * NB + threadIdx.x];
     __syncthreads();
+    if (threadIdx.x == 0) bulk_load(&lamB[0][0][0], pn.lam + (size_t)m * NB * NB, NB * NB * sizeof(double), &bar);
+    if (threadIdx.x < NB) s_r[threadIdx.x] = pn.rd[(size_t)m * NB + threadIdx.x];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane >> 2, q = lane & 3;
     const int I = blockIdx.x * PANEL_WARPS + warp;
-    if (I >= nt) return;
     const int p0 = NB * round, K0 = KB * round;
+    const bool inP = I >= K0 && I < K0 + KB;
+    const int i = 8 * I + r;
+    double v[MC];  // A[i, p0 + 4mc + q] (A fragments), in flight while Lam lands
+#pragma unroll
+    for (int mc = 0; mc < MC; ++mc) v[mc] = (I < nt && !inP) ? md.a[sym_index(i, p0 + 4 * mc + q)] : 0.0;
+    const bool landed = mbar_wait_bounded(&bar, 0);
+    if (!__syncthreads_and(landed)) {  // every thread leaves here together
+        if (threadIdx.x == 0) atomicMax(md.stat, MGPU_ERR_TIMEOUT);
+        mbar_wait_bounded(&bar, 0);  // let the copy land before the CTA's shared memory goes
+        return;
+    }
+    if (I >= nt) return;
     double *xf = pn.xf + ((size_t)m * nt + I) * MC * 32;
     double *bf = pn.bf + ((size_t)m * nt + I) * MC * 32;
-    if (I >= K0 && I < K0 + KB) {
+    if (inP) {
         // rows of P: X(p0+a, k) = Lam[k][a] / delta_k, B(p0+a, k) = -Lam[k][a]
         const int a = 8 * (I - K0) + r;
         for (int mc = 0; mc < MC; ++mc) {
             const int kk = 4 * mc + q;
-            const double la = lam[kk * NB + a];
+            const double la = lamB[kk >> 3][a >> 2][((kk & 7) << 2) | (a & 3)];
             xf[mc * 32 + lane] = la * s_r[kk];
             bf[mc * 32 + lane] = -la;
         }
@@ -337,10 +353,6 @@ big_panel_kernel(const MatDesc *__restrict__ mds, Panels pn, int nt, int round, 
     double acc[KB][2];
 #pragma unroll
     for (int kt = 0; kt < KB; ++kt) acc[kt][0] = acc[kt][1] = 0.0;
-    const int i = 8 * I + r;
-    double v[MC];  // A[i, p0 + 4mc + q] (A fragments), all loads in flight together
-#pragma unroll
-    for (int mc = 0; mc < MC; ++mc) v[mc] = md.a[sym_index(i, p0 + 4 * mc + q)];
     // Lam is unit lower triangular: output columns 8kt..8kt+7 need k-steps mc <= 2kt+1 only
 #pragma unroll
     for (int mc = 0; mc < MC; ++mc)
