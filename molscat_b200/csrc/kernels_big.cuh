@@ -85,10 +85,11 @@ __device__ __forceinline__ size_t sym_index(int i, int j)
     return (size_t)tix(R >> 3, C >> 3) * 64 + ((R & 7) * 4 + ((C & 7) >> 1)) * 2 + (C & 1);
 }
 
-// tile t -> (I, J), I >= J
+// tile t -> (I, J), I >= J.  8t + 1 is exact in single precision (t < 2^21,
+// NT <= 128 gives t < 8256); the loops correct the rounded root by one either way.
 __device__ __forceinline__ void tile_ij(int t, int &I, int &J)
 {
-    int i = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    int i = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
     while (i * (i + 1) / 2 > t) --i;
     while ((i + 1) * (i + 2) / 2 <= t) ++i;
     I = i;
