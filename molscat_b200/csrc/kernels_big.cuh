@@ -527,23 +527,80 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldmd_pre_kernel(StepArgs a)
     v[2 * a.npad + i] = y23;
 }
 
+// W(R) of the element pair (i, j), (i, j + 1) at tiled offsets 2p, 2p + 1:
+// HAMMAT + SUMLAM (hammat.f:85-113, sumlam.f:74-86) with the arithmetic of
+// cta::w_elem, both elements from one 16-byte load per term.
+__device__ __forceinline__ double2 w_pair(const SysDev &S, const double *__restrict__ P, size_t p, int i, int j, int ir,
+                                          double ered)
+{
+    const size_t tdp = (size_t)S.ntiles * 32;  // pairs per coupling term
+    double w0 = 0.0, w1 = 0.0;
+    const double2 *vl = reinterpret_cast<const double2 *>(S.vlt) + p;
+    if (S.ivlfl <= 0) {
+        for (int l = 0; l < S.nham; ++l) {
+            const double2 v = __ldg(vl + l * tdp);
+            const double pl = __ldg(P + l);
+            w0 = fma(v.x, pl, w0);
+            w1 = fma(v.y, pl, w1);
+        }
+    } else {
+        const int2 *iv = reinterpret_cast<const int2 *>(S.ivt) + p;
+        for (int l = 0; l < S.nham; ++l) {
+            const double2 v = __ldg(vl + l * tdp);
+            const int2 ix = __ldg(iv + l * tdp);
+            if (v.x != 0.0) w0 = fma(v.x, __ldg(P + ix.x), w0);
+            if (v.y != 0.0) w1 = fma(v.y, __ldg(P + ix.y), w1);
+        }
+    }
+    const int d = (i == j) ? 0 : (i == j + 1) ? 1 : -1;  // which element is on the diagonal
+    if (d >= 0 && i < S.n) {
+        double w = d ? w1 : w0;
+        const double R = __ldg(S.rtab + ir);
+        const double rsq = fmin(1.0 / (R * R), 1.0e16);
+        if (S.nrsq == 0) w += rsq * S.cent[i];
+        if (S.nconst == 0) w += S.eint[i];
+        if (S.conlen > 0.0) {
+            const double c2 = S.conlen * S.conlen;
+            w += R * R / (c2 * c2);
+        }
+        w -= ered;
+        if (d) w1 = w; else w0 = w;
+    }
+    return make_double2(w0, w1);
+}
+
+// pair p of a tiled matrix -> row i and first column j (the pair is (i, j), (i, j + 1))
+__device__ __forceinline__ void pair_ij(size_t p, int &i, int &j)
+{
+    int I, J;
+    tile_ij((int)(p >> 5), I, J);
+    const int l = (int)p & 31;
+    i = 8 * I + (l >> 2);
+    j = 8 * J + 2 * (l & 3);
+}
+
 // Y = 2HQ(C_k) + 2 Y14 - Y23 Y^-1 Y23  (tiles hold -Y^-1; mdprop.f:156,181-185)
 __global__ void __launch_bounds__(EW_THREADS) big_ldmd_mid_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];  // by value: the stores below cannot alias it
     const MatDesc md = a.md[m];
     const int k = *a.kstep;
     if (k > md.nstep) return;
     const double *v = a.vec + (size_t)m * 3 * a.npad;
-    const double *qk = S.q + (size_t)(k - 1) * a.td;
-    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+    const double2 *qk = reinterpret_cast<const double2 *>(S.q + (size_t)(k - 1) * a.td);
+    double2 *y = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
         int i, j;
-        elem_ij(x, i, j);
-        double w = __ldg(qk + x) + v[2 * a.npad + i] * md.a[x] * v[2 * a.npad + j];
-        if (i == j) w += 2.0 * v[i];
-        md.a[x] = w;
+        pair_ij(p, i, j);
+        const double2 q = __ldg(qk + p), yp = y[p];
+        const double v23i = v[2 * a.npad + i];
+        double w0 = q.x + v23i * yp.x * v[2 * a.npad + j];
+        double w1 = q.y + v23i * yp.y * v[2 * a.npad + j + 1];
+        if (i == j) w0 += 2.0 * v[i];
+        if (i == j + 1) w1 += 2.0 * v[i];
+        y[p] = make_double2(w0, w1);
     }
 }
 
@@ -552,7 +609,7 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldmd_post_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];  // by value: the stores below cannot alias it
     const MatDesc md = a.md[m];
     const int k = *a.kstep;
     if (k > md.nstep) return;
@@ -560,12 +617,17 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldmd_post_kernel(StepArgs a)
     const double dd = (k == S.nstep) ? d1 : d2;
     const double *v = a.vec + (size_t)m * 3 * a.npad;
     const double *P = ptab_row(S, 2 * k);
-    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+    double2 *y = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
         int i, j;
-        elem_ij(x, i, j);
-        double w = dd * cta::w_elem(S, P, (int)x, i, j, 2 * k, job.ered, true) + v[2 * a.npad + i] * md.a[x] * v[2 * a.npad + j];
-        if (i == j) w += v[a.npad + i];
-        md.a[x] = w;
+        pair_ij(p, i, j);
+        const double2 w = w_pair(S, P, p, i, j, 2 * k, job.ered), yp = y[p];
+        const double v23i = v[2 * a.npad + i];
+        double r0 = dd * w.x + v23i * yp.x * v[2 * a.npad + j];
+        double r1 = dd * w.y + v23i * yp.y * v[2 * a.npad + j + 1];
+        if (i == j) r0 += v[a.npad + i];
+        if (i == j + 1) r1 += v[a.npad + i];
+        y[p] = make_double2(r0, r1);
     }
 }
 
