@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldmd_init_kernel(StepArgs a, c
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *md.cnt = 0;
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldmd_pre_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     const int k = *a.kstep;
     if (k > md.nstep) return;
@@ -636,7 +636,7 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldj_init_kernel(StepArgs a, co
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *md.cnt = 0;
@@ -661,17 +661,19 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldj_pre_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     const int k = *a.kstep;
     if (k > md.nstep) return;
     const double h = S.dr / 2.0, d4 = -h * h / 48.0;
-    double *u = a.tiles2 + (size_t)m * a.td;
+    double2 *u = reinterpret_cast<double2 *>(a.tiles2 + (size_t)m * a.td);
     const double *P = ptab_row(S, 2 * k - 1);
-    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
         int i, j;
-        elem_ij(x, i, j);
-        u[x] = d4 * cta::w_elem(S, P, (int)x, i, j, 2 * k - 1, job.ered, true) + ((i == j && i < S.n) ? 0.125 : 0.0);
+        pair_ij(p, i, j);
+        const double2 w = w_pair(S, P, p, i, j, 2 * k - 1, job.ered);
+        u[p] = make_double2(d4 * w.x + ((i == j && i < S.n) ? 0.125 : 0.0),
+                            d4 * w.y + ((i == j + 1 && i < S.n) ? 0.125 : 0.0));
     }
 }
 
@@ -680,14 +682,17 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldj_mid_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     if (*a.kstep > md.nstep) return;
-    const double *u = a.tiles2 + (size_t)m * a.td;
-    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+    const double2 *u = reinterpret_cast<const double2 *>(a.tiles2 + (size_t)m * a.td);
+    double2 *z = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
         int i, j;
-        elem_ij(x, i, j);
-        md.a[x] = -u[x] + md.a[x] - ((i == j && i < S.n) ? 6.0 : 0.0);
+        pair_ij(p, i, j);
+        const double2 up = u[p], zp = z[p];
+        z[p] = make_double2(-up.x + zp.x - ((i == j && i < S.n) ? 6.0 : 0.0),
+                            -up.y + zp.y - ((i == j + 1 && i < S.n) ? 6.0 : 0.0));
     }
 }
 
@@ -696,18 +701,20 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldj_post_kernel(StepArgs a)
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     const int k = *a.kstep;
     if (k > md.nstep) return;
     const double h = S.dr / 2.0, d1 = h * h / 3.0, d2 = 2.0 * d1;
     const double dd = (k == S.nstep) ? d1 : d2;
     const double *P = ptab_row(S, 2 * k);
-    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+    double2 *z = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
         int i, j;
-        elem_ij(x, i, j);
-        md.a[x] = dd * cta::w_elem(S, P, (int)x, i, j, 2 * k, job.ered, true) + ((i == j && i < S.n) ? 2.0 : 0.0) +
-                  md.a[x];
+        pair_ij(p, i, j);
+        const double2 w = w_pair(S, P, p, i, j, 2 * k, job.ered), zp = z[p];
+        z[p] = make_double2(dd * w.x + ((i == j && i < S.n) ? 2.0 : 0.0) + zp.x,
+                            dd * w.y + ((i == j + 1 && i < S.n) ? 2.0 : 0.0) + zp.y);
     }
 }
 
@@ -720,7 +727,7 @@ big_finish_kernel(StepArgs a, int ldj, double *__restrict__ y, int *__restrict__
 {
     const int m = blockIdx.y;
     const JobDev job = a.jobs[m];
-    const SysDev &S = a.sys[job.sys];
+    const SysDev S = a.sys[job.sys];
     const MatDesc md = a.md[m];
     const int st = *md.stat;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -755,7 +762,7 @@ __global__ void big_step_advance_kernel(int *kstep, int value)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(EW_THREADS) big_prep_build_kernel(const SysDev *__restrict__ sys, int s, int k0, size_t td)
 {
-    const SysDev &S = sys[s];
+    const SysDev S = sys[s];
     const int k = k0 + blockIdx.y;
     if (k > S.nstep) return;
     const double h = S.dr / 2.0, d4 = -h * h / 48.0;
@@ -770,7 +777,7 @@ __global__ void __launch_bounds__(EW_THREADS) big_prep_build_kernel(const SysDev
 
 __global__ void __launch_bounds__(EW_THREADS) big_prep_finish_kernel(const SysDev *__restrict__ sys, int s, int k0, size_t td)
 {
-    const SysDev &S = sys[s];
+    const SysDev S = sys[s];
     const int k = k0 + blockIdx.y;
     if (k > S.nstep) return;
     double *u = S.q + (size_t)(k - 1) * td;
