@@ -1,4 +1,5 @@
-// LDMD / LDJ for large N (NPAD = 64*m, 256 <= NPAD <= 1024): the matrices of
+// LDMD / LDJ for large N (NPAD = 64*m <= 1024; N above 200 by default, any N
+// when this family is selected for an N range): the matrices of
 // a batch live in global memory (L2 / HBM) as lower 8x8 tiles in the DMMA
 // accumulator layout of warp_dmma.cuh (tile t = I(I+1)/2 + J, lane l holds
 // (8I + l/4, 8J + 2(l%4) + s)).  Included by propagator.cu after
@@ -8,14 +9,16 @@
 // pivots a round (one tile row/column block P of 8 tiles), in three batched
 // kernels per round over all matrices of the batch:
 //   factor  one CTA per matrix: unpivoted LDL^T of D = A_PP (lower triangle
-//           only), Lam = L^{-1} and 1/delta_k, negative pivots counted
-//           (SYMINV's KOUNT, syminv.f:27-49);
-//   panel   every 8-row block: c = A[i, P] Lam^T on DMMA, written as the
+//           only), Lam = L^{-1} (in the panel's fragment order) and
+//           1/delta_k, negative pivots counted (SYMINV's KOUNT, syminv.f:27-49);
+//   panel   every 8-row block: Lam by one bulk copy, c = A[i, P] Lam^T on DMMA, written as the
 //           update operands X = -c/delta, B = c (rows of P: X = Lam^T/delta,
 //           B = -Lam^T) in A-fragment order;
 //   update  every lower tile: tiles of row/column block P zeroed, then
 //           A_IJ += X_I B_J^T on DMMA (64 k-steps of m8n8k4), X and B staged
-//           in shared memory by bulk (TMA) copies.
+//           in shared memory by bulk (TMA) copies; split into the next
+//           round's diagonal block, the rest of its block row and column,
+//           and everything else (the look-ahead).
 // which leaves A_ij - sum_k c_k(i) c_k(j)/delta_k outside P, A_iP D^{-1} in
 // the columns of P and -D^{-1} in A_PP, the scalar sweep's values.  All reads
 // take the lower triangle, so rounding left in the upper halves of diagonal
