@@ -88,3 +88,26 @@ def test_gpu_bound_states_equal_oracle(basic1):
     ora = _states(bp, sysm, g, counter=oracle_counts)
     for (_, e), (_, o) in zip(got, ora):
         assert abs(e - o) <= 1e-9 * abs(o) + 2 * TOL_CM
+
+
+def test_bisection_brackets_every_state_with_a_counting_stub():
+    """The search logic alone (bd.driver.f:993-1054): a stub count with known
+    levels stands in for the propagations; every state between EMIN and EMAX
+    is found once, numbered by the count below it, within tol."""
+    levels = np.array([-7.25, -3.5, -3.4999, -1.0, 0.75])
+    calls = []
+
+    def stub(bp, ereds):
+        e = np.asarray(ereds, dtype=np.float64)
+        calls.append(e.size)
+        return np.searchsorted(levels, e, side="left")  # states strictly below E
+
+    tol = 1.0e-9
+    found = find_states(None, -5.0, 1.0, tol, counter=stub)
+    inside = levels[(levels > -5.0) & (levels < 1.0)]
+    assert [k for k, *_ in found] == [1, 2, 3, 4]
+    for (k, e, lo, hi), lev in zip(found, inside):
+        assert hi - lo <= tol and lo <= lev <= hi
+        assert abs(e - lev) <= tol
+    # every round puts all unresolved states' trial energies into one batch
+    assert calls[0] == 2 and max(calls[1:]) <= len(inside)
