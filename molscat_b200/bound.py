@@ -106,6 +106,34 @@ def node_counts(bp: BoundProblem, ereds) -> tuple:
         plan.close()
 
 
+def bisect_steps(count: Callable, lo: float, hi: float, c_lo: int, c_hi: int, tol: float,
+                 max_rounds: int = 200) -> list:
+    """Every step of a monotone count between lo and hi, bisected until its
+    bracket is narrower than tol; every live bracket's midpoint goes into one
+    call of count(xs) -> counts per round.  Returns [(k, x, lo, hi)] for the
+    step between counts k and k + 1, at the bracket midpoint.  An increasing
+    count (c_hi > c_lo) is BOUND's in energy; a decreasing one is FIELD's
+    case of levels rising with the field (fld.driver.f:864-881)."""
+    inc = c_hi >= c_lo
+    brackets = {k: [lo, hi] for k in range(min(c_lo, c_hi), max(c_lo, c_hi))}
+    for _ in range(max_rounds):
+        live = [k for k, (a, b) in brackets.items() if b - a > tol]
+        if not live:
+            break
+        mids = np.array([0.5 * (brackets[k][0] + brackets[k][1]) for k in live])
+        counts = count(mids)
+        for x, cnt in zip(mids, counts):
+            # tighten every bracket this point informs
+            for kk, br in brackets.items():
+                if br[0] < x < br[1]:
+                    below = (cnt <= kk) if inc else (cnt > kk)  # the step lies above x
+                    if below:
+                        br[0] = x
+                    else:
+                        br[1] = x
+    return [(k, 0.5 * (a + b), a, b) for k, (a, b) in sorted(brackets.items())]
+
+
 def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_rounds: int = 200,
                 counter: Callable | None = None) -> list:
     """Every state with EMIN < E < EMAX (reduced energies), bisected until its
@@ -115,19 +143,4 @@ def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_roun
     counts` defaults to the GPU node count."""
     count = counter or (lambda b, e: node_counts(b, e)[0])
     c0, c1 = (int(x) for x in count(bp, [emin, emax]))
-    brackets = {k: [emin, emax] for k in range(c0, c1)}
-    for _ in range(max_rounds):
-        live = [k for k, (lo, hi) in brackets.items() if hi - lo > tol]
-        if not live:
-            break
-        mids = np.array([0.5 * (brackets[k][0] + brackets[k][1]) for k in live])
-        counts = count(bp, mids)
-        for k, e, cnt in zip(live, mids, counts):
-            # tighten every bracket this energy informs
-            for kk, br in brackets.items():
-                if br[0] < e < br[1]:
-                    if cnt <= kk:
-                        br[0] = e
-                    else:
-                        br[1] = e
-    return [(k, 0.5 * (lo + hi), lo, hi) for k, (lo, hi) in sorted(brackets.items())]
+    return bisect_steps(lambda xs: count(bp, xs), emin, emax, c0, c1, tol, max_rounds)

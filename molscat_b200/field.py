@@ -1,0 +1,81 @@
+"""Fields at which bound states cross a fixed energy (FIELD's search,
+fld.driver.f), with the propagations batched on the GPU.
+
+At a fixed energy E the number of bound states below E changes with an
+external field F as the levels move with it.  FIELD counts states at FLDMIN
+and FLDMAX, assumes the count changes monotonically in between and seeks
+|NODES(FLDMAX) - NODES(FLDMIN)| states (fld.driver.f:855-881), each by
+bisection on the field (fld.driver.f:889-1060).  The count at one field is
+BOUND's: NODES_out + NODES_in + the non-positive eigenvalues of
+Y_out - Y_in at RMATCH (bdctrl.f:197,221-257).
+
+A trial field is its own coupled-channel system: the caller's
+coupling_at(F) returns the channel thresholds (and couplings) at F, which
+FIELD obtains through SETEFV / CHEINT (fld.driver.f:926-935).  Every trial
+field of a bisection round goes into one batched plan (outward and inward
+segments of all fields together), so one GPU launch set serves all states.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Callable
+
+import numpy as np
+
+from .bound import adiabatic_wkb_y, bisect_steps
+from .propagators import Coupling, Plan, Segment
+
+
+@dataclass
+class FieldProblem:
+    """One (JTOT, block) at one energy, with its field-dependent coupling."""
+    coupling_at: Callable[[float], Coupling]
+    seg_out: Segment  # RMIN -> RMATCH
+    seg_in: Segment   # RMAX -> RMATCH (DR < 0)
+    ered: float
+    prop: str = "LDMD"
+    y_out0: Callable[[Coupling], np.ndarray] | None = None
+    y_in0: Callable[[Coupling], np.ndarray] | None = None
+
+    def __post_init__(self):
+        so, si, e = self.seg_out, self.seg_in, self.ered
+        if self.y_out0 is None:
+            self.y_out0 = lambda c: adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
+        if self.y_in0 is None:
+            self.y_in0 = lambda c: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
+
+
+def field_node_counts(fp: FieldProblem, fields) -> tuple:
+    """(counts, NODES_out, NODES_in, matching counts) at every field, all
+    fields' propagations in one plan."""
+    fields = np.asarray(fields, dtype=np.float64)
+    m = fields.size
+    cs = [fp.coupling_at(float(f)) for f in fields]
+    job_sys = np.arange(2 * m, dtype=np.int32)
+    plan = Plan(fp.prop, cs + cs, [fp.seg_out] * m + [fp.seg_in] * m, job_sys, np.full(2 * m, fp.ered))
+    try:
+        y0 = [fp.y_out0(c) for c in cs] + [fp.y_in0(c) for c in cs]
+        ybuf, nodes, status, kfail = plan.run_host(plan.pack(y0))
+        if (status != 0).any():
+            j = int(np.nonzero(status)[0][0])
+            raise RuntimeError(f"propagation failed at F={fields[j % m]} (status {int(status[j])}, "
+                               f"step {int(kfail[j])})")
+        nmatch = np.array([int(np.sum(np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k)) <= 0.0))
+                           for k in range(m)], dtype=np.int64)
+        n_out = nodes[:m].astype(np.int64)
+        n_in = nodes[m:].astype(np.int64)
+        return n_out + n_in + nmatch, n_out, n_in, nmatch
+    finally:
+        plan.close()
+
+
+def find_fields(fp: FieldProblem, fmin: float, fmax: float, tol: float, max_rounds: int = 200,
+                counter: Callable | None = None) -> list:
+    """Every field in (FMIN, FMAX) where a state crosses the energy, bisected
+    until its bracket is narrower than tol.  Returns [(k, field, lo, hi)]:
+    the crossing where the count of states below the energy steps between k
+    and k + 1 (up or down with the field, whichever the end counts say).
+    `counter(fp, fields) -> counts` defaults to the GPU node count."""
+    count = counter or (lambda p, f: field_node_counts(p, f)[0])
+    c0, c1 = (int(x) for x in count(fp, [fmin, fmax]))
+    return bisect_steps(lambda xs: count(fp, xs), fmin, fmax, c0, c1, tol, max_rounds)
