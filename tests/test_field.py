@@ -78,3 +78,7 @@ def test_gpu_field_counts_equal_oracle(basic1):
     assert len(got) == len(want)
     for f, w in zip(got, want):
         assert abs(f - w) < REF_TOL_CM, (f, w)
+    # the same fields as the oracle's search, within 1e-9 relative
+    ora = sorted(f for _, f, _, _ in find_fields(fp, fmin, fmax, TOL_CM, counter=oracle_field_counts))
+    for f, o in zip(got, ora):
+        assert abs(f - o) <= 1e-9 * abs(o) + 2 * TOL_CM, (f, o)
