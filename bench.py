@@ -51,9 +51,10 @@ def parse():
                     help="batch: the batched rotor workload (default); serve: the request server under "
                          "Poisson arrivals of mixed-N solves")
     ap.add_argument("--requests", type=int, default=3000, help="serve: requests in the timed stream")
-    ap.add_argument("--rate", type=float, default=20000.0, help="serve: Poisson arrival rate, requests/s")
+    ap.add_argument("--rate", type=float, default=None,
+                    help="serve: Poisson arrival rate, requests/s (default: half the saturated capacity)")
     ap.add_argument("--nmin", type=int, default=16)
-    ap.add_argument("--nmax", type=int, default=256)
+    ap.add_argument("--nmax", type=int, default=1024)
     ap.add_argument("--serve-nstep", type=int, default=1000, help="serve: steps per propagation")
     ap.add_argument("--serve-systems", type=int, default=32)
     ap.add_argument("--streams", type=int, default=4)
@@ -61,6 +62,16 @@ def parse():
     ap.add_argument("--large-n", default="256,512,1024", help="large: channel counts of the dense systems")
     ap.add_argument("--large-energies", type=int, default=64)
     ap.add_argument("--large-nstep", type=int, default=3000)
+    # the serving and large-N legs of the default run (1 GPU): short, fixed sizes
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg of the default run")
+    ap.add_argument("--no-large", action="store_true", help="skip the large-N leg of the default run")
+    ap.add_argument("--leg-serve-requests", type=int, default=240)
+    ap.add_argument("--leg-serve-nstep", type=int, default=400)
+    ap.add_argument("--leg-serve-systems", type=int, default=24)
+    ap.add_argument("--leg-plain-sample", type=int, default=12)
+    ap.add_argument("--leg-large-n", default="512,1024")
+    ap.add_argument("--leg-large-energies", type=int, default=64)
+    ap.add_argument("--leg-large-nstep", type=int, default=300)
     return ap.parse_args()
 
 
@@ -125,27 +136,55 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 # CPU side: the oracle (a C restatement of the reference path) as baseline
 # ----------------------------------------------------------------------------
-def _cpu_worker(args):
-    os.environ["OPENBLAS_NUM_THREADS"] = "1"
-    jt, block, energy_cm = args
-    sys.path.insert(0, ROOT)
-    from oracle import oracle as O
+_CPU_GRID = {}
+
+
+def _cpu_grid():
+    """The rotor workload's radial grid and P table (identical for every
+    (JTOT, block)); built once per process."""
+    if not _CPU_GRID:
+        from oracle import oracle as O
+        from molscat_b200 import systems as S
+        sysm = S.rotor_system()
+        rmin, rmax = S.ROTOR_RMIN_A / sysm.rm, S.ROTOR_RMAX_A / sysm.rm
+        nstep = S.ROTOR_NSTEP
+        dr = (rmax - rmin) / nstep
+        rtab = O.radial_grid(rmin, dr, nstep)
+        ptab = O.ptable(O.Itype1(ured=sysm.ured, be=sysm.be, jlevel=list(sysm.jlevel), lam=list(sysm.lam),
+                                 terms=[list(t) for t in sysm.terms], rm=sysm.rm, epsil=sysm.epsil), rtab)
+        _CPU_GRID.update(nstep=nstep, dr=dr, rtab=rtab, ptab=ptab, cm2ru=sysm.cm2ru)
+    return _CPU_GRID
+
+
+def _cpu_inputs(job):
+    """Everything one oracle propagation of (JTOT, block, E) needs, built
+    outside any timed region: the coupling arrays and the WKB start."""
     from molscat_b200 import systems as S
-    sysm = S.rotor_system()
-    c = sysm.coupling(jt, block)
-    rmin, rmax = S.ROTOR_RMIN_A / sysm.rm, S.ROTOR_RMAX_A / sysm.rm
-    nstep = S.ROTOR_NSTEP
-    dr = (rmax - rmin) / nstep
-    rtab = O.radial_grid(rmin, dr, nstep)
-    ptab = O.ptable(O.Itype1(ured=sysm.ured, be=sysm.be, jlevel=list(sysm.jlevel), lam=list(sysm.lam),
-                             terms=[list(t) for t in sysm.terms], rm=sysm.rm, epsil=sysm.epsil), rtab)
-    oc = O.Coupling(n=c.n, nham=c.nham, vl=c.vl, eint=c.eint, cent=c.cent)
-    ered = energy_cm * sysm.cm2ru
-    y0 = S.wkb_initial_y(c, ptab[0], rtab[0], ered)
+    jt, block, energy_cm = job
+    g = _cpu_grid()
+    c = S.rotor_system().coupling(jt, block)
+    ered = energy_cm * g["cm2ru"]
+    y0 = S.wkb_initial_y(c, g["ptab"][0], g["rtab"][0], ered)
+    return (c.n, c.nham, c.vl, c.eint, c.cent, ered, y0)
+
+
+def _cpu_pool_init():
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    sys.path.insert(0, ROOT)
+    _cpu_grid()
+
+
+def _cpu_propagate(inp):
+    """One oracle MDPROP propagation; returns (N^3*NSTEP, seconds, status)."""
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    from oracle import oracle as O
+    n, nham, vl, eint, cent, ered, y0 = inp
+    g = _cpu_grid()
+    oc = O.Coupling(n=n, nham=nham, vl=vl, eint=eint, cent=cent)
     t0 = time.perf_counter()
-    _, nodes, st, _ = O.mdprop(oc, rtab, ptab, nstep, dr, ered, y0)
+    _, nodes, st, _ = O.mdprop(oc, g["rtab"], g["ptab"], g["nstep"], g["dr"], ered, y0)
     dt = time.perf_counter() - t0
-    return c.n ** 3 * nstep, dt, st
+    return n ** 3 * g["nstep"], dt, st
 
 
 def cpu_sample_jobs(count: int, seed: int = 7):
@@ -160,13 +199,15 @@ def cpu_sample_jobs(count: int, seed: int = 7):
 
 
 def cpu_baseline_serial(budget_s: float):
-    """Single-thread oracle on a bounded sample of the workload."""
+    """Single-thread oracle on a bounded sample of the workload (inputs built
+    before each propagation is timed)."""
     from oracle import oracle as O
     O.build()
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
     work = tsum = 0.0
     jobs = 0
     for job in cpu_sample_jobs(400):
-        w, dt, st = _cpu_worker(job)
+        w, dt, st = _cpu_propagate(_cpu_inputs(job))
         work += w
         tsum += dt
         jobs += 1
@@ -174,12 +215,17 @@ def cpu_baseline_serial(budget_s: float):
             break
     return {"value": work / tsum, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{jobs} full 4000-step MDPROP propagations drawn from the batch, oracle C restatement "
-                      f"(unpivoted SYMINV N<=30, scipy-OpenBLAS DSYTRF/DSYTRI N>30), 1 thread, {tsum:.1f} s"}
+                      f"(unpivoted SYMINV N<=30, scipy-OpenBLAS DSYTRF/DSYTRI N>30), 1 thread, {tsum:.1f} s "
+                      "of propagation (coupling, P table and WKB start built outside the timed region)"}
 
 
 def run_reference(args):
     """--impl reference: the reference path's CPU implementation (the oracle
-    port; the Fortran reference cannot be compiled here) on all host cores."""
+    port; the Fortran reference cannot be compiled here) on all host cores.
+    Each step propagates 4 x `cores` jobs sampled from the batch, handed to
+    the processes one at a time;
+    the inputs (couplings, P table, WKB start) are built before the timed
+    region, so only the propagations and the pool's dispatch are timed."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -188,15 +234,16 @@ def run_reference(args):
     O.build()
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
-    per_step = cores
+    per_step = 4 * cores  # several jobs per process and step, dealt one at a time: balanced load
     samples = cpu_sample_jobs(per_step * (args.steps + args.warmup), seed=11)
     times = []
     work_total = 0.0
-    with ctx.Pool(cores) as pool:
+    with ctx.Pool(cores, initializer=_cpu_pool_init) as pool:
+        inputs = pool.map(_cpu_inputs, samples)
         for s in range(args.warmup + args.steps):
-            chunk = samples[s * per_step:(s + 1) * per_step]
+            chunk = inputs[s * per_step:(s + 1) * per_step]
             t0 = time.perf_counter()
-            res = pool.map(_cpu_worker, chunk)
+            res = pool.map(_cpu_propagate, chunk, chunksize=1)
             dt = time.perf_counter() - t0
             if any(r[2] != 0 for r in res):
                 raise RuntimeError("oracle propagation failed")
@@ -213,8 +260,8 @@ def run_reference(args):
                                f"{per_step} propagations sampled from the JTOT=0..80 x 2 parities x 512 energies batch",
                    "parallelism": f"{cores} host processes"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{per_step} full propagations per step, spawn pool of {cores} processes, "
-                                   "OpenBLAS 1 thread each"},
+                         "sample": f"{per_step} full propagations per step, spawn pool of {cores} processes (jobs dealt one at a time), "
+                                   "OpenBLAS 1 thread each; inputs built before the timed region"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -283,106 +330,121 @@ def dominant_bucket(wl, lo=33, hi=40):
             np.array([wl.job_ered[j] for j in jobs]), [wl.job_y0[j] for j in jobs])
 
 
-def run_serve(args):
-    """Request server under a seeded Poisson stream of single MDPROP solves,
-    N log-uniform in [nmin, nmax] over a pool of dense synthetic systems
-    registered (device-resident, 2HQ(C) prepared) before the timed region.
-    Beside it, the plain one-solve-at-a-time GPU loop (mgpu_mdprop per
-    request: plan, preparation and propagation every call) on a sample of the
-    same requests."""
+def serve_leg(requests: int, rate: float | None, nmin: int, nmax: int, nstep: int, nsys: int, streams: int,
+              plain_sample: int, seed: int = 20261203) -> dict:
+    """Request server under seeded single MDPROP solves, N log-uniform in
+    [nmin, nmax] over a pool of dense synthetic systems registered
+    (device-resident, 2HQ(C) prepared) before the timed region.
+
+    Two passes over fresh draws of `requests` solves: a saturated one (every
+    request submitted at once) gives the capacity, then a Poisson stream at
+    `rate` requests/s (None: half the measured capacity) gives the latency
+    percentiles.  Beside them the plain one-solve-at-a-time GPU loop
+    (mgpu_mdprop per request: plan, preparation and propagation each call) on
+    the first `plain_sample` saturated requests, whose results must equal the
+    served ones bit for bit."""
     import math
     import numpy as np
-    import torch
-    from molscat_b200.build import build
-    build()
     from molscat_b200 import systems as S
     from molscat_b200.propagators import propagate
     from molscat_b200.serving import Server, latency_percentiles
-    torch.cuda.set_device(0)
-    from molscat_b200 import autotune
-    tuned = autotune.apply(autotune.default_path("LDMD")) if os.path.exists(autotune.default_path("LDMD")) else 0
-    rng = np.random.default_rng(20261203)
-    K = args.serve_systems
-    ns = np.exp(rng.uniform(math.log(args.nmin), math.log(args.nmax), K)).astype(int)
-    pool = [S.synthetic_system(int(n), args.serve_nstep, seed=1000 + k) for k, n in enumerate(ns)]
-    R = args.requests
-    pick = rng.integers(0, K, R)
-    de = rng.uniform(0.0, 10.0, R)
-    arrive = np.cumsum(rng.exponential(1.0 / args.rate, R))
-    srv = Server("LDMD", hbm_budget=48 << 30, streams=args.streams, max_batch=4096, max_systems=K)
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(nmin), math.log(nmax), nsys)).astype(int)
+    pool = [S.synthetic_system(int(n), nstep, seed=1000 + k) for k, n in enumerate(ns)]
+    srv = Server("LDMD", hbm_budget=48 << 30, streams=streams, max_batch=4096, max_systems=nsys)
     ids = [srv.add_system(c, seg) for (c, seg, _, _) in pool]
-    for k in range(K):  # first use of every bucket's kernels
+    for k in range(nsys):  # first use of every bucket's kernels
         srv.submit(ids[k], pool[k][2], pool[k][3]).wait()
+
+    def stream(count, arrive):
+        pick = rng.integers(0, nsys, count)
+        de = rng.uniform(0.0, 10.0, count)
+        t0 = time.perf_counter()
+        reqs = []
+        for i in range(count):
+            if arrive is not None:
+                while time.perf_counter() - t0 < arrive[i]:
+                    pass
+            k = int(pick[i])
+            reqs.append(srv.submit(ids[k], pool[k][2] + de[i], pool[k][3]))
+        for r in reqs:
+            r.wait()
+        wall = max(r.times()[2] for r in reqs) - min(r.times()[0] for r in reqs)
+        work = float(sum(int(ns[int(k)]) ** 3 * nstep for k in pick))
+        return reqs, pick, de, wall, work
+
     clocks = ClockSampler(0)
     clocks.start()
-    t0 = time.perf_counter()
-    reqs = []
-    for i in range(R):
-        while time.perf_counter() - t0 < arrive[i]:
-            pass
-        k = int(pick[i])
-        reqs.append(srv.submit(ids[k], pool[k][2] + de[i], pool[k][3]))
-    for r in reqs:
-        r.wait()
+    sreqs, spick, sde, swall, swork = stream(requests, None)
+    cap = requests / swall
+    rate = rate or 0.5 * cap
+    arrive = np.cumsum(rng.exponential(1.0 / rate, requests))
+    preqs, _, _, pwall, pwork = stream(requests, arrive)
     clk = clocks.stop()
-    t_first = min(r.times()[0] for r in reqs)
-    t_last = max(r.times()[2] for r in reqs)
-    wall = t_last - t_first
-    work = float(sum(int(ns[int(k)]) ** 3 * args.serve_nstep for k in pick))
-    lat = latency_percentiles(reqs, (50, 90, 99))
-    # the plain loop on the first requests, and equality of their results
-    ns_plain = min(args.plain_sample, R)
+    lat = latency_percentiles(preqs, (50, 90, 99))
+    lat_sat = latency_percentiles(sreqs, (50, 99))
+    nplain = min(plain_sample, requests)
     same = True
     tp = time.perf_counter()
-    for i in range(ns_plain):
-        k = int(pick[i])
+    for i in range(nplain):
+        k = int(spick[i])
         c, seg, e, y0 = pool[k]
-        y, nodes = propagate("LDMD", c, seg, e + de[i], y0)
-        same = same and bool(np.array_equal(y, reqs[i].wait())) and nodes == reqs[i].nodes
+        y, nodes = propagate("LDMD", c, seg, e + sde[i], y0)
+        same = same and bool(np.array_equal(y, sreqs[i].wait())) and nodes == sreqs[i].nodes
     tp = time.perf_counter() - tp
-    work_plain = float(sum(int(ns[int(pick[i])]) ** 3 * args.serve_nstep for i in range(ns_plain)))
+    work_plain = float(sum(int(ns[int(spick[i])]) ** 3 * nstep for i in range(nplain)))
     srv.close()
-    line = {
-        "metric": "channel^3*steps/s (served single MDPROP solves, mixed N)", "value": work / wall,
-        "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-        "solves_per_s": R / wall, "latency_s": lat,
-        "plain_loop": {"value": work_plain / tp, "unit": UNIT, "solves_per_s": ns_plain / tp,
-                       "sample": f"first {ns_plain} requests, mgpu_mdprop one at a time"},
-        "served_over_plain": (work / wall) / (work_plain / tp), "results_equal_plain": same,
-        "config": {"workload": f"Poisson arrivals {args.rate:.0f}/s, {R} requests, N log-uniform "
-                               f"{args.nmin}-{args.nmax} over {K} dense synthetic systems (NHAM 6), "
-                               f"{args.serve_nstep} steps each, energies jittered per request",
-                   "streams": args.streams, "hbm_budget_gb": 48,
-                   "registration": "systems registered and 2HQ(C) prepared before the timed region",
-                   "tuning": f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"},
+    return {
+        "value": swork / swall, "unit": UNIT, "solves_per_s": cap,
+        "latency_s": lat, "offered_rate_per_s": rate, "poisson_solves_per_s": requests / pwall,
+        "poisson_value": pwork / pwall, "saturated_latency_s": lat_sat,
+        "plain_loop": {"value": work_plain / tp, "unit": UNIT, "solves_per_s": nplain / tp,
+                       "sample": f"first {nplain} saturated requests, mgpu_mdprop one at a time"},
+        "served_over_plain": (swork / swall) / (work_plain / tp), "results_equal_plain": same,
+        "config": {"workload": f"{requests} saturated then {requests} Poisson-arrival single MDPROP solves, "
+                               f"N log-uniform {nmin}-{nmax} over {nsys} dense synthetic systems (NHAM 6), "
+                               f"{nstep} steps each, energies jittered per request",
+                   "streams": streams, "hbm_budget_gb": 48,
+                   "registration": "systems registered and 2HQ(C) prepared before the timed region"},
         "clocks": clk,
     }
-    print(json.dumps(line), flush=True)
 
 
-def run_large(args):
-    """Large dense N: one dense synthetic system per N (NHAM 6 Lennard-Jones
-    terms, seeded), `large_energies` energies each, MDPROP over `large_nstep`
-    steps; all systems in one plan (their buckets run concurrently), then each
-    N alone.  FP64 TFLOP/s of the propagation phase against the measured peak."""
-    import numpy as np
+def run_serve(args):
+    """--workload serve: the serving leg alone, with its own flags."""
     import torch
     from molscat_b200.build import build
     build()
+    torch.cuda.set_device(0)
+    from molscat_b200 import autotune
+    tuned = autotune.apply(autotune.default_path("LDMD")) if os.path.exists(autotune.default_path("LDMD")) else 0
+    out = serve_leg(args.requests, args.rate, args.nmin, args.nmax, args.serve_nstep, args.serve_systems,
+                    args.streams, args.plain_sample)
+    out["config"]["tuning"] = f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"
+    line = {"metric": "channel^3*steps/s (served single MDPROP solves, mixed N)", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic", **out}
+    print(json.dumps(line), flush=True)
+
+
+def large_leg(ns, energies: int, nstep: int, reps: int, peak: float | None = None) -> dict:
+    """Large dense N: one dense synthetic system per N (NHAM 6 Lennard-Jones
+    terms, seeded), `energies` energies each, MDPROP over `nstep` steps; all
+    systems in one plan (their buckets run concurrently), then each N alone.
+    FP64 TFLOP/s of the propagation phase (CUDA events on the launching
+    stream, 2HQ(C) prepared before) against the measured FP64 peak."""
+    import numpy as np
+    import torch
     from molscat_b200 import systems as S
     from molscat_b200.propagators import Plan
-    torch.cuda.set_device(0)
-    ns = [int(x) for x in args.large_n.split(",")]
-    E = args.large_energies
-    sysd = [S.synthetic_system(n, args.large_nstep, seed=600 + n) for n in ns]
+    sysd = [S.synthetic_system(n, nstep, seed=600 + n) for n in ns]
 
     def timed(idx):
         systems = [sysd[i][0] for i in idx]
         segs = [sysd[i][1] for i in idx]
-        job_sys = np.repeat(np.arange(len(idx), dtype=np.int32), E)
-        job_e = np.concatenate([sysd[i][2] + np.linspace(0.0, 10.0, E) for i in idx])
+        job_sys = np.repeat(np.arange(len(idx), dtype=np.int32), energies)
+        job_e = np.concatenate([sysd[i][2] + np.linspace(0.0, 10.0, energies) for i in idx])
         plan = Plan("LDMD", systems, segs, job_sys, job_e)
-        y0 = torch.from_numpy(plan.pack([sysd[i][3] for i in idx for _ in range(E)])).cuda()
+        y0 = torch.from_numpy(plan.pack([sysd[i][3] for i in idx for _ in range(energies)])).cuda()
         y = torch.empty_like(y0)
         nd = torch.zeros(plan.njobs, dtype=torch.int32, device="cuda")
         st, kf = torch.zeros_like(nd), torch.zeros_like(nd)
@@ -393,7 +455,7 @@ def run_large(args):
         if (st.cpu().numpy() != 0).any():
             raise RuntimeError("large-N propagation failed")
         ms = []
-        for _ in range(max(1, args.steps)):
+        for _ in range(max(1, reps)):
             y.copy_(y0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
@@ -403,30 +465,47 @@ def run_large(args):
             ms.append(e0.elapsed_time(e1))
         t = statistics.mean(ms)
         out = {"ms": t, "tflops": plan.flops_prop / (t * 1e-3) / 1e12,
-               "channel3_steps_per_s": sum(ns[i] ** 3 * args.large_nstep for i in idx) * E / (t * 1e-3)}
+               "channel3_steps_per_s": sum(ns[i] ** 3 * nstep for i in idx) * energies / (t * 1e-3)}
         plan.close()
+        del y0, y
+        torch.cuda.empty_cache()
         return out
 
     clocks = ClockSampler(0)
     clocks.start()
-    allr = timed(list(range(len(ns))))
+    allr = timed(list(range(len(ns)))) if len(ns) > 1 else None
     alone = {str(ns[i]): timed([i]) for i in range(len(ns))}
     clk = clocks.stop()
-    dgemm, dfma = fp64_peaks(torch)
-    peak = max(dgemm, dfma)
-    for r in [allr] + list(alone.values()):
+    src = "given"
+    if peak is None:
+        dgemm, dfma = fp64_peaks(torch)
+        peak = max(dgemm, dfma)
+        src = "max(cuBLAS DGEMM 8192^3 %.1f, DFMA probe %.1f) TFLOP/s measured in this run (of measured)" % (
+            dgemm / 1e12, dfma / 1e12)
+    for r in ([allr] if allr else []) + list(alone.values()):
         r["frac"] = r["tflops"] * 1e12 / peak
-    line = {"metric": "FP64 TFLOP/s (batched large-N MDPROP propagation)", "value": allr["tflops"],
-            "unit": "TFLOP/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "fp64_frac": allr["frac"], "channel3_steps_per_s": allr["channel3_steps_per_s"], "per_n": alone,
-            "peak_tflops": peak / 1e12,
-            "peak_source": "max(cuBLAS DGEMM 8192^3 %.1f, DFMA probe %.1f) TFLOP/s measured in this run (of measured)"
-                           % (dgemm / 1e12, dfma / 1e12),
-            "config": {"workload": f"dense synthetic systems N={ns} (NHAM 6), {E} energies each, "
-                                   f"{args.large_nstep} MDPROP steps; all N in one plan (buckets concurrent), "
-                                   "then each N alone; propagation phase timed (2HQ(C) prepared before)",
-                       "steps": args.steps},
+    return {"value": (allr or alone[str(ns[0])])["tflops"], "unit": "TFLOP/s",
+            "fp64_frac": (allr or alone[str(ns[0])])["frac"], "per_n": alone, "peak_tflops": peak / 1e12,
+            "peak_source": src,
+            "algorithmic": "2N^3 + 2 NHAM N(N+1) flops per propagation step (two Y inversions + W(B))",
+            "config": {"workload": f"dense synthetic systems N={list(ns)} (NHAM 6), {energies} energies each, "
+                                   f"{nstep} MDPROP steps; " + ("all N in one plan (buckets concurrent), then "
+                                                               if len(ns) > 1 else "") +
+                                   "each N alone; propagation phase timed (2HQ(C) prepared before)",
+                       "reps": reps},
             "clocks": clk}
+
+
+def run_large(args):
+    """--workload large: the large-N leg alone, with its own flags."""
+    import torch
+    from molscat_b200.build import build
+    build()
+    torch.cuda.set_device(0)
+    ns = [int(x) for x in args.large_n.split(",")]
+    out = large_leg(ns, args.large_energies, args.large_nstep, args.steps)
+    line = {"metric": "FP64 TFLOP/s (batched large-N MDPROP propagation)", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f64", "data": "synthetic", **out}
     print(json.dumps(line), flush=True)
 
 
@@ -630,11 +709,24 @@ def main():
             "cpu_baseline": cpu,
             "setup_s": t_setup,
         }
+    plan.close()
+    del y0_dev, y_dev
+    torch.cuda.empty_cache()
+    if rank == 0 and world == 1:
+        # the rest of the metric: served mixed-N solves (capacity, p50/p99
+        # latency, against the plain one-at-a-time loop) and large dense N
+        if not args.no_serve:
+            line["serving"] = serve_leg(args.leg_serve_requests, None, 16, 1024, args.leg_serve_nstep,
+                                        args.leg_serve_systems, args.streams, args.leg_plain_sample)
+        if not args.no_large:
+            ns = [int(x) for x in args.leg_large_n.split(",")]
+            line["large_n"] = large_leg(ns, args.leg_large_energies, args.leg_large_nstep, 2, peak=peak)
+            line["large_n"]["peak_source"] = line["roofline"]["peak_source"]
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    plan.close()
 
 
 if __name__ == "__main__":
