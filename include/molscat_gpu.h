@@ -161,6 +161,12 @@ double mgpu_plan_flops_phase(const mgpu_plan *plan, int phases);
  * checksum so the work cannot be optimised away. */
 int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_out);
 
+/* The pivot reciprocal every inversion uses (a third-order Newton refinement
+ * of the hardware seed, exact power-of-two scaling), applied to n doubles:
+ * r_dev[i] = 1/x_dev[i] within one ulp for normal results.  Device buffers;
+ * asynchronous on `stream`.  For tests of that claim. */
+int mgpu_probe_pivot_reciprocal(const double *x_dev, double *r_dev, int n, void *stream);
+
 /* ---- allocation-free variant ---------------------------------------------
  * mgpu_mdprop_noalloc: MDPROP for njobs energies of one system that makes no
  * device allocation at all.  It has no counterpart in the reference.
@@ -180,15 +186,27 @@ int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_
  *
  * Instead of allocating, the library uses one fixed 64 MiB scratch array,
  * reserved on every GPU that loads the library until the process exits.  A
- * request that needs more (about 128*NSTEP*NT*(NT+1)/2 bytes for the per-step
- * 2HQ(C) table, NT = ceil(N/4)), more than 4096 jobs or N above 200 (the
- * large-N kernels need per-job device matrices) is rejected with
- * MGPU_ERR_UNSUPPORTED.  All calls share that array and it keeps the last
- * call's contents (each call rewrites what it reads and zeroes its counters),
- * so calls that overlap on the GPU -- on different streams or from different
- * host threads -- race with each other: serialise them.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) and
- * should be made before any stream capture. */
+ * request that needs more, more than 4096 jobs or N above 200 (the large-N
+ * kernels need per-job device matrices) is rejected with
+ * MGPU_ERR_UNSUPPORTED.  Most of a request's scratch is the per-step 2HQ(C)
+ * table: 512*NSTEP*NT*(NT+1)/2 bytes, NT = the 8x8 tile count of N's kernel
+ * bucket (ceil(N/8) for N <= 64; 10, 12, 14, 16, 20 or 25 above, the
+ * smallest that holds ceil(N/8)); the VL tiles, 512*NHAM*NT*(NT+1)/2 bytes
+ * (half again with IVLFL > 0), and a few KB of descriptors come on top.  So
+ * N = 36 fits about 8,600 steps and N = 200 about 400.
+ *
+ * All calls share that array and it keeps the last call's contents (each
+ * call rewrites what it reads and zeroes its counters), so calls that overlap
+ * on the GPU -- on different streams or from different host threads -- race
+ * with each other: serialise them.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it for the life of
+ * the process; make that first call before any stream capture, and make no
+ * call after a cudaDeviceReset on that device (the address may be stale).
+ *
+ * An IV entry outside 1..NHAM (IVLFL > 0) is not checked on the host, since
+ * IV lives in device memory here: it turns the coupling into NaN, so every
+ * job reports MGPU_ERR_NONFINITE with step 1 (mgpu_plan_create rejects the
+ * same input with MGPU_ERR_ARG). */
 int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, int njobs,
                         const double *ered_dev, double *y_dev, int *nodes_dev,
                         int *status_dev, int *kfail_dev, void *stream);

@@ -48,7 +48,7 @@ EXPORTS = (
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
     "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
     "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
-    "mgpu_plan_run_host_smatrix",
+    "mgpu_plan_run_host_smatrix", "mgpu_probe_pivot_reciprocal",
 )
 
 _lib = None
@@ -85,6 +85,7 @@ def load(path: str | None = None):
     L.mgpu_plan_flops_phase.argtypes = [vp, ctypes.c_int]
     L.mgpu_plan_flops_phase.restype = ctypes.c_double
     L.mgpu_probe_fp64_fma.argtypes = [vp, ctypes.c_int, vp, _dp]
+    L.mgpu_probe_pivot_reciprocal.argtypes = [vp, vp, ctypes.c_int, vp]
     L.mgpu_mdprop_noalloc.argtypes = [pc, pg, ctypes.c_int, vp, vp, vp, vp, vp, vp]
     L.mgpu_status_string.argtypes = [ctypes.c_int]
     L.mgpu_status_string.restype = ctypes.c_char_p

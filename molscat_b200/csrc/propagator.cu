@@ -582,6 +582,13 @@ __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double *out, int it
     if (acc == 12345.678) out[0] = acc;  // practically never true; keeps the chains live
 }
 
+// pivot_reciprocal on a vector, for the test that holds it to 1.0/x
+__global__ void __launch_bounds__(256) pivot_reciprocal_probe_kernel(const double *x, double *r, int n)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = pivot_reciprocal(x[i]);
+}
+
 // ---------------------------------------------------------------------------
 // bucket dispatch
 // ---------------------------------------------------------------------------
@@ -1368,6 +1375,16 @@ int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_
     fp64_fma_probe_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(out_dev, iters);
     if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "probe launch", e);
     if (flops_out) *flops_out = 2.0 * 8.0 * 16.0 * (double)iters * 256.0 * (double)blocks;
+    return MGPU_OK;
+}
+
+int mgpu_probe_pivot_reciprocal(const double *x_dev, double *r_dev, int n, void *stream)
+{
+    if (!x_dev || !r_dev || n < 0) return set_err(MGPU_ERR_ARG, "probe arguments");
+    if (n == 0) return MGPU_OK;
+    pivot_reciprocal_probe_kernel<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(x_dev, r_dev, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(MGPU_ERR_CUDA, "probe launch", e);
     return MGPU_OK;
 }
 

@@ -1,9 +1,12 @@
 """Extract golden S matrices and bound-state energies from the reference's
 example outputs.
 
-Run in a checkout that has the reference project at $MOLSCAT_REF (default
-/root/reference); writes tests/golden/molscat_all_propagators.json and
-tests/golden/bound_basic1.json.  The fixtures are committed, so nothing at
+Run with the reference project's checkout named by $MOLSCAT_REF (required):
+
+    MOLSCAT_REF=<path to molscat checkout> python tests/golden/make_golden.py
+
+writes tests/golden/molscat_all_propagators.json,
+tests/golden/bound_basic1.json and tests/golden/bound_ar_ch4.json.  The fixtures are committed, so nothing at
 test time reads the reference tree.
 
 Bound states: examples/output/bound-basic1.output (the same model system,
@@ -21,9 +24,12 @@ import os
 import re
 import sys
 
-REF = os.environ.get("MOLSCAT_REF", "/root/reference")
+REF = os.environ.get("MOLSCAT_REF")
+if not REF:
+    sys.exit("set MOLSCAT_REF to the reference project's checkout")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "molscat_all_propagators.json")
 OUT_BOUND = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_basic1.json")
+OUT_ARCH4 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_ar_ch4.json")
 
 
 def parse_runs(text):
@@ -96,6 +102,56 @@ def main_bound():
     print("wrote", OUT_BOUND, file=sys.stderr)
 
 
+def main_ar_ch4():
+    """bound-Ar_CH4: ITYPE=6 (CH4 as a spherical top with centrifugal
+    distortion, the MSV potential of Buck et al. through its VSTAR plug-in),
+    JTOT=1 block 2, MDPROP outward from RMIN (IRMSET=8) to RMATCH and inward
+    from RMAX, DR=0.01.  The system is read from the input file: the &BASIS
+    and &POTL values and the five VINIT data lines."""
+    with open(os.path.join(REF, "examples", "input", "bound-Ar_CH4.input")) as f:
+        inp = f.read()
+
+    def num(name):
+        return float(re.search(name + r"\s*=\s*([-+0-9.Ee]+)", inp).group(1))
+
+    roti = [float(x) for x in re.search(r"ROTI\s*=\s*(.*?)JMAX", inp, re.S).group(1)
+            .replace(",", " ").split()]
+    lam = [int(x) for x in re.search(r"LAMBDA\s*=\s*([0-9, ]+)", inp).group(1).replace(",", " ").split()]
+    mxlam = int(num("MXLAM"))
+    data = [[float(x) for x in ln.split()] for ln in inp.split("/")[-1].strip().splitlines()]
+    with open(os.path.join(REF, "examples", "output", "bound-Ar_CH4.output")) as f:
+        text = f.read()
+    pairs = [{"state": int(m[0]), "j": int(m[1]), "tau": int(m[2]), "prty": int(m[3]), "energy_cm": float(m[7])}
+             for m in re.findall(r"^\s+(\d+)\s+(\d+)\s+(-?\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+(\S+)\s*$",
+                                 text.split("PAIR STATE    ---")[1].split("=====")[0], re.M)]
+    # CHANNEL, PAIR STATE, J, TAU, PRTY, two more state numbers, L, PAIR LEVEL, PAIR ENERGY
+    chans = [(int(m[1]), int(m[7])) for m in re.findall(
+        r"^\s+(\d+)\s+(\d+)\s+(\d+)\s+(-?\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+(\d+)\s+(\S+)\s*$",
+        text.split("CHANNEL FUNCTION LIST:")[1].split("NODE COUNT")[0], re.M)]
+    states = [{"state": int(a), "energy_cm": float(b)} for a, b in
+              re.findall(r"CONVERGED ON STATE NUMBER\s+(\d+)\s+AT\s+ENERGY =\s+(\S+)\s+CM-1", text)]
+    doc = {
+        "source": "examples/input/bound-Ar_CH4.input, examples/output/bound-Ar_CH4.output (pair states, "
+                  "channel list, converged states)",
+        "system": {
+            "itype": 6, "ured": num("URED"), "roti": roti, "jmax": int(num("JMAX")), "isym": int(num("ISYM")),
+            "lambda": [[lam[2 * i], lam[2 * i + 1]] for i in range(mxlam)],
+            "epsil": data[0][0], "rm": data[0][1], "beta": data[1], "c6c8": data[2], "x1234": data[3],
+            "alphas": data[4:4 + mxlam - 1],
+            "jtot": int(num("JTOTL")), "block": int(num("IBFIX")), "rmin": num("RMIN"), "rmatch": num("RMATCH"),
+            "rmax": num("RMAX"), "dr": num("DR"), "irmset": int(num("IRMSET")), "emin_cm": num("EMIN"),
+            "emax_cm": num("EMAX"), "convergence_cm": 1.0e-7,
+        },
+        "pair_states": pairs,
+        "channels": [{"pair_state": a, "l": b} for a, b in chans],
+        "states": states,
+    }
+    with open(OUT_ARCH4, "w") as f:
+        json.dump(doc, f, indent=1)
+    print("wrote", OUT_ARCH4, file=sys.stderr)
+
+
 if __name__ == "__main__":
     main()
     main_bound()
+    main_ar_ch4()

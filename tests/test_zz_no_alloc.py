@@ -82,7 +82,7 @@ def _run_plan(c, seg, ereds, y0s):
 
 
 def test_noalloc_matches_plan_on_two_calls_in_a_row(torch_cuda):
-    # first call N=36 (nine 4x4 tile rows), second call N=15: the second one
+    # first call N=36 (five 8x8 tile rows), second call N=15: the second one
     # must not see anything the first left in the shared scratch array
     for jtot, block, nstep, energies in ((10, 2, 300, (120.0, 300.0, 480.0)), (4, 1, 200, (60.0, 250.0))):
         c, seg, jobs = cases.rotor_case(jtot, block, nstep=nstep, energies_cm=energies)
@@ -96,6 +96,33 @@ def test_noalloc_matches_plan_on_two_calls_in_a_row(torch_cuda):
             assert np.abs(u - v).max() / max(1.0, np.abs(v).max()) < Y_TOL
 
 
+@pytest.mark.parametrize("n, ivlfl, nconst", [(100, 1, 1), (60, 0, 0)], ids=["cta-iv", "cta"])
+def test_noalloc_cta_bucket_matches_plan_on_two_calls_in_a_row(torch_cuda, n, ivlfl, nconst):
+    # one CTA per matrix (40 < N <= 200), with the IV indexing converted to
+    # the tile layout on the device; two calls in a row with different
+    # energies, each against the plan entry point
+    c, seg, ered, y0 = cases.random_case(n, 120, seed=4100 + n, ivlfl=ivlfl, nconst=nconst)
+    for ereds in ((ered, ered + 3.0), (ered + 7.5,)):
+        y0s = [y0] * len(ereds)
+        ya, na, sa = _run_noalloc(torch_cuda, c, seg, ereds, y0s)
+        yb, nb, sb = _run_plan(c, seg, ereds, y0s)
+        assert (sa == 0).all() and (sb == 0).all()
+        assert np.array_equal(na, nb)
+        for u, v in zip(ya, yb):
+            assert np.abs(u - v).max() / max(1.0, np.abs(v).max()) < Y_TOL
+
+
+def test_noalloc_bad_iv_reports_nonfinite(torch_cuda):
+    # IV lives in device memory, so an index outside 1..NHAM is not checked
+    # on the host: the device turns it into NaN couplings and every job
+    # reports MGPU_ERR_NONFINITE at step 1
+    c, seg, ered, y0 = cases.random_case(12, 20, seed=4200, ivlfl=1)
+    c.iv = c.iv.copy()
+    c.iv[0] = c.nham + 5
+    _, _, st = _run_noalloc(torch_cuda, c, seg, [ered], [y0])
+    assert (st == _lib.MGPU_ERR_NONFINITE).all()
+
+
 def test_noalloc_rejects_requests_beyond_the_scratch_limit(torch_cuda):
     L = _lib.load()
     c, seg, _ = cases.rotor_case(10, 2, nstep=10)
@@ -103,7 +130,8 @@ def test_noalloc_rejects_requests_beyond_the_scratch_limit(torch_cuda):
                     ctypes.cast(1 << 20, ctypes.POINTER(ctypes.c_int)),
                     ctypes.cast(1 << 20, ctypes.POINTER(ctypes.c_double)),
                     ctypes.cast(1 << 20, ctypes.POINTER(ctypes.c_double)))
-    # N=36 needs 5760 bytes of 2HQ(C) per step: 20000 steps exceed 64 MiB
+    # N=36 (five 8x8 tile rows) needs 512*15 = 7680 bytes of 2HQ(C) per
+    # step: 20000 steps exceed 64 MiB
     gs = Grid_C(20000, 0.001, ctypes.cast(1 << 20, ctypes.POINTER(ctypes.c_double)),
                 ctypes.cast(1 << 20, ctypes.POINTER(ctypes.c_double)))
     vp = ctypes.c_void_p
