@@ -13,6 +13,7 @@ example outputs:
 * power/exponential P(R) ........ source_code/potenl.f (evaluation case 1)
 * HAMMAT scaling of P ........... source_code/hammat.f:31-83
 * FINDRM (IRMSET>0) ............. source_code/findrm.f:1-259
+* ITYPE=6 basis, couplings ...... oracle/itype6.py (asrot.f, set6c.f, set6.f)
 * DRSET fixed step .............. source_code/drset.f:29-84
 * CALCK / GTWVEC / CHNSRT ....... calck.f, gtwvec.f, chnsrt.f
 * YINIT (adiabatic, WKB) ........ source_code/yinit.f:66-150
@@ -343,20 +344,29 @@ def lowest_adiabat(sysm, c: Coupling, r: float, ered: float) -> float:
     return float(np.linalg.eigvalsh(w)[0])
 
 
-def findrm(sysm, c: Coupling, rstart: float, ered: float, irmset: int = 9):
-    """FINDRM for MOLSCAT (findrm.f:43-250).  Returns (RSTART, RTURN)."""
+def findrm(sysm, c: Coupling, rstart: float, ered: float, irmset: int = 9, bound: bool = False):
+    """FINDRM (findrm.f:43-250).  Returns (RSTART, RTURN).  MOLSCAT starts
+    the secant search from the smallest centrifugal turning point of the open
+    channels (findrm.f:40-57); BOUND and FIELD (bound=True) start it at the
+    input RSTART with one try only (findrm.f:31-38).  Where the reference's
+    BOUND branch would fall back to its (unset) RMIN, this returns the input
+    RSTART."""
     rmin = rstart
-    rturn = 1.0e30
-    for i in range(c.n):
-        dif = ered - c.eint[i]
-        if dif < 0.0:
-            continue
-        rcent = math.sqrt(c.cent[i] / dif)
-        rcent = max(rcent, rmin)
-        rturn = min(rturn, rcent)
-    itry = 0
-    if rturn == rmin:
+    if bound:
+        rturn = rstart
         itry = 1
+    else:
+        rturn = 1.0e30
+        for i in range(c.n):
+            dif = ered - c.eint[i]
+            if dif < 0.0:
+                continue
+            rcent = math.sqrt(c.cent[i] / dif)
+            rcent = max(rcent, rmin)
+            rturn = min(rturn, rcent)
+        itry = 0
+        if rturn == rmin:
+            itry = 1
     while True:  # label 10
         itry += 1
         rstart = rturn

@@ -128,3 +128,63 @@ def rel_err(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.abs(a - b).max() / max(1.0, np.abs(b).max()))
+
+
+# ---------------------------------------------------------------------------
+# large dense N on a physical basis: atom + rigid asymmetric top (ITYPE=6)
+# ---------------------------------------------------------------------------
+ASYM_ROTI = (9.6, 0.0, 4.3, 0.0, 2.8, 0.0, 0.0, 0.0, 0.0, 0.0)  # A, B, C (cm-1)
+ASYM_LAMBDA = [(0, 0), (1, 0), (2, 0), (2, 2), (3, 2), (4, 4)]
+ASYM_URED = 12.0
+ASYM_R = (2.8, 30.0)  # Angstrom (RM = 1 Angstrom)
+# (level cutoff cm-1, JTOT, block, channels kept): below 400 cm-1 the largest
+# block has 500 channels, so the N = 1024 block takes levels below 700 cm-1
+ASYM_BLOCKS = {256: (400.0, 4, 1, 256), 512: (400.0, 10, 2, 500), 1024: (700.0, 10, 1, 1024)}
+
+
+def asym_top_system(emax_cm: float, seed: int = 20261203):
+    """The large-N workload's physical basis: an asymmetric top (A 9.6,
+    B 4.3, C 2.8 cm-1) with its levels below emax_cm, and six V(lambda, mu)
+    Lennard-Jones 12-6 terms with seeded well depths 5-40 cm-1 (the
+    isotropic term the deepest) and minima 3.6-4.0 Angstrom."""
+    from oracle import itype6 as I6
+    rng = np.random.default_rng(seed)
+    amp = np.sort(rng.uniform(5.0, 40.0, len(ASYM_LAMBDA)))[::-1].copy()
+    rmn = rng.uniform(3.6, 4.0, len(ASYM_LAMBDA))
+
+    def pfunc(r):
+        x = rmn / r
+        return amp * (x ** 12 - 2.0 * x ** 6)
+
+    return I6.Itype6(ured=ASYM_URED, roti=ASYM_ROTI, jmax=30, lam=ASYM_LAMBDA, pfunc=pfunc, rm=1.0, epsil=1.0,
+                     emax=emax_cm)
+
+
+def asym_top_case(n_target: int, nstep: int, energies_cm=(150.0,), seed: int = 20261203):
+    """(Coupling, Segment, [(ERED, Y0)], system) of the N ~ n_target block:
+    MDPROP from 2.8 to 30 Angstrom in nstep steps, Y0 the diagonal WKB start."""
+    from oracle import oracle as O
+    emax, jtot, block, nmax = ASYM_BLOCKS[n_target]
+    sysm = asym_top_system(emax, seed)
+    oc = sysm.coupling(jtot, block, nmax=nmax)
+    c = Coupling(n=oc.n, nham=oc.nham, vl=oc.vl, eint=oc.eint, cent=oc.cent)
+    r0, r1 = ASYM_R
+    dr = (r1 - r0) / nstep
+    rtab = radial_grid(r0, dr, nstep)
+    seg = Segment(nstep, dr, rtab, O.ptable(sysm, rtab))
+    jobs = []
+    for e in energies_cm:
+        ered = e * sysm.cm2ru
+        jobs.append((ered, S.wkb_initial_y(c, seg.ptab[0], seg.rtab[0], ered)))
+    return c, seg, jobs, sysm
+
+
+def smatrix(c, y, r: float, ered: float):
+    """S = (SR, SI) from Y at the last radius by the oracle's YTOK/KTOS, in
+    CHNSRT order (open channels first); returns (SR, SI, NOPEN)."""
+    from oracle import oracle as O
+    wvec, nopen = O.gtwvec(ered, c.eint)
+    nb = O.chnsrt(c.eint)
+    k = O.ytok(nb, wvec, c.n, nopen, y, r, c.cent)
+    sr, si = O.ktos(k)
+    return sr, si, nopen
