@@ -6,7 +6,8 @@ Run with the reference project's checkout named by $MOLSCAT_REF (required):
     MOLSCAT_REF=<path to molscat checkout> python tests/golden/make_golden.py
 
 writes tests/golden/molscat_all_propagators.json,
-tests/golden/bound_basic1.json and tests/golden/bound_ar_ch4.json.  The fixtures are committed, so nothing at
+tests/golden/bound_basic1.json, tests/golden/bound_ar_ch4.json and
+tests/golden/molscat_ityp6.json.  The fixtures are committed, so nothing at
 test time reads the reference tree.
 
 Bound states: examples/output/bound-basic1.output (the same model system,
@@ -30,6 +31,8 @@ if not REF:
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "molscat_all_propagators.json")
 OUT_BOUND = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_basic1.json")
 OUT_ARCH4 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_ar_ch4.json")
+OUT_ITYP6 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "molscat_ityp6.json")
+ITYP6_JTOTS = (0, 1, 2, 5, 10, 20, 30, 40, 60, 80)
 
 
 def parse_runs(text):
@@ -151,7 +154,56 @@ def main_ar_ch4():
     print("wrote", OUT_ARCH4, file=sys.stderr)
 
 
+def main_ityp6():
+    """molscat-ityp6: ITYPE=6 spherical top (as bound-Ar_CH4 but ISYM=224,
+    JMAX=9), LDMD from RMIN (IRMSET=8) to RMID = 1.3 x RTURN, AIRY from RMID
+    to RMAX (TOLHI=1e-4), one energy (300 cm-1); the printed state-to-state
+    partial cross sections of the JTOT values in ITYP6_JTOTS, both blocks."""
+    with open(os.path.join(REF, "examples", "input", "molscat-ityp6.input")) as f:
+        inp = f.read()
+
+    def num(name):
+        return float(re.search(r"\b" + name + r"\s*=\s*([-+0-9.Ee]+)", inp).group(1))
+
+    roti = [float(x) for x in re.search(r"ROTI\s*=\s*(.*?)JMAX", inp, re.S).group(1).replace(",", " ").split()]
+    lam = [int(x) for x in re.search(r"LAMBDA\s*=\s*([0-9, ]+)", inp).group(1).replace(",", " ").split()]
+    mxlam = int(num("MXLAM"))
+    data = [[float(x) for x in ln.split()] for ln in inp.split("/")[-1].strip().splitlines()]
+    with open(os.path.join(REF, "examples", "output", "molscat-ityp6.output")) as f:
+        text = f.read()
+    blocks = []
+    parts = re.split(r"ANGULAR MOMENTUM JTOT\s*=\s*(\d+)\s+AND SYMMETRY BLOCK\s*=\s*(\d+)", text)
+    for jt, blk, body in zip(parts[1::3], parts[2::3], parts[3::3]):
+        if int(jt) not in ITYP6_JTOTS:
+            continue
+        tab = body.split("FOR JTOT =")[1] if "PARTIAL CROSS SECTIONS" in body else ""
+        m = re.search(r"F\s+I =([\d ]+)\n((?:\s+\d+(?:\s+\S+E[-+]\d+)+\n)+)", tab)
+        if not m:
+            continue
+        levels = [int(x) for x in m.group(1).split()]
+        rows = [ln.split() for ln in m.group(2).strip("\n").split("\n")]
+        sig = [{"final": int(r[0]), "initial": levels[k], "sigma": float(v)}
+               for r in rows for k, v in enumerate(r[1:])]
+        blocks.append({"jtot": int(jt), "block": int(blk), "sigma": sig})
+    doc = {
+        "source": "examples/input/molscat-ityp6.input, examples/output/molscat-ityp6.output (state-to-state "
+                  "partial cross sections)",
+        "system": {
+            "itype": 6, "ured": num("URED"), "roti": roti, "jmax": int(num("JMAX")), "isym": int(num("ISYM")),
+            "lambda": [[lam[2 * i], lam[2 * i + 1]] for i in range(mxlam)],
+            "epsil": data[0][0], "rm": data[0][1], "beta": data[1], "c6c8": data[2], "x1234": data[3],
+            "alphas": data[4:4 + mxlam - 1], "rmin": num("RMIN"), "rmax": num("RMAX"), "steps": num("STEPS"),
+            "irmset": int(num("IRMSET")), "rvfac": num("RVFAC"), "tolhi": num("TOLHI"), "energy_cm": num("ENERGY"),
+        },
+        "blocks": blocks,
+    }
+    with open(OUT_ITYP6, "w") as f:
+        json.dump(doc, f, indent=1)
+    print("wrote", OUT_ITYP6, file=sys.stderr)
+
+
 if __name__ == "__main__":
     main()
     main_bound()
     main_ar_ch4()
+    main_ityp6()

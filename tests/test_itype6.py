@@ -21,6 +21,15 @@ inward from RMAX, DR = 0.01, four bound states in -100..-60 cm-1.
   NODES exact, Y(RSTOP) within 5e-8 relative to max|Y| (diagonal, first
   column, Frobenius norm), S within 1e-8 absolute (first four columns), and
   the GPU's S unitary within 1e-8.
+* molscat-ityp6 (examples/input/molscat-ityp6.input, examples/output/
+  molscat-ityp6.output; fixture by make_golden.py): the same molecule with
+  ISYM = 224, LDMD from RMIN (IRMSET = 8) to RMID = 1.3 RTURN and AIRY
+  (oracle/aiprop.py) to RMAX, 300 cm-1.  The oracle alone reproduces the
+  printed state-to-state partial cross sections (six digits) for JTOT = 0..80,
+  N = 2..59; with the GPU propagating the LDMD segment (N = 39..59, above
+  the reference's N = 30 switch from SYMINV to DSYTRF/DSYNEG) the same
+  printed values come out, with Y(RMID) within 5e-8 of the oracle's and
+  NODES equal.
 """
 import json
 import os
@@ -158,3 +167,78 @@ def test_asym_top_large_n_against_oracle(large_golden, gpu, n_target):
     assert np.abs(si[:, :m].T - np.array(run["si_cols"])).max() < S_TOL
     s = sr + 1j * si
     assert np.abs(s @ s.conj().T - np.eye(nopen)).max() < S_TOL
+
+
+# ---------------------------------------------------------------------------
+# molscat-ityp6: LDMD to RMID, AIRY to RMAX, state-to-state cross sections
+# ---------------------------------------------------------------------------
+def _ityp6_system():
+    from oracle import itype6 as I6
+    with open(os.path.join(HERE, "golden", "molscat_ityp6.json")) as f:
+        g = json.load(f)
+    s = g["system"]
+    pot = I6.BuckMSV(*s["beta"], *s["c6c8"], *s["x1234"], [tuple(a) for a in s["alphas"]],
+                     [lm for lm, _ in s["lambda"][1:]])
+    sysm = I6.Itype6(ured=s["ured"], roti=tuple(s["roti"]), jmax=s["jmax"], lam=[tuple(x) for x in s["lambda"]],
+                     pfunc=pot, rm=s["rm"], epsil=s["epsil"], isym=s["isym"])
+    return g, sysm
+
+
+def _ityp6_block(g, sysm, blk, short_range=None):
+    from oracle import aiprop as A
+    s = g["system"]
+    ch = sysm.channels(blk["jtot"], blk["block"])
+    c = sysm.coupling(blk["jtot"], blk["block"])
+    res = A.molscat_two_segment(sysm, c, s["energy_cm"], s["rmin"], s["rmax"], s["steps"], s["irmset"], s["rvfac"],
+                                s["tolhi"], short_range=short_range)
+    return c, res, A.partial_cross_sections(sysm, c, ch, res, blk["jtot"])
+
+
+def _check_sigma(xs, blk):
+    # six significant digits printed: half a unit of the sixth digit, plus an
+    # absolute floor for entries at the rounding-noise level of the block
+    big = max(x["sigma"] for x in blk["sigma"])
+    for x in blk["sigma"]:
+        got = xs[(x["final"], x["initial"])]
+        assert abs(got - x["sigma"]) <= 6e-6 * x["sigma"] + 1e-9 * big, (blk["jtot"], blk["block"], x, got)
+
+
+@pytest.mark.parametrize("jtot", [0, 1, 2, 5, 10, 20, 30, 40, 60, 80])
+def test_ityp6_oracle_cross_sections_match_reference(jtot):
+    """The oracle alone (MDPROP + AIRY): N = 2..59."""
+    g, sysm = _ityp6_system()
+    for blk in g["blocks"]:
+        if blk["jtot"] == jtot:
+            _check_sigma(_ityp6_block(g, sysm, blk)[2], blk)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("jtot", [5, 10, 20, 40, 60, 80])
+def test_ityp6_gpu_short_range_matches_reference(gpu, jtot):
+    """The GPU propagates the LDMD segment (N = 39..59, past the reference's
+    N > 30 switch to DSYTRF/DSYNEG), the oracle's AIRY the long range: the
+    reference's printed cross sections, the oracle's Y(RMID) within 5e-8 and
+    its NODES exactly."""
+    from oracle import oracle as O
+    from molscat_b200.propagators import propagate
+    g, sysm = _ityp6_system()
+    for blk in g["blocks"]:
+        if blk["jtot"] != jtot:
+            continue
+        seen = {}
+
+        def gpu_ldmd(rtab, ptab, nstep, dr, ered, y0, c_holder=seen):
+            oc = c_holder["c"]
+            c = Coupling(n=oc.n, nham=oc.nham, vl=oc.vl, eint=oc.eint, cent=oc.cent)
+            y, nodes = propagate("LDMD", c, Segment(nstep, dr, rtab, ptab), ered, y0)
+            yo, no, st, _ = O.mdprop(oc, rtab, ptab, nstep, dr, ered, y0)
+            assert st == 0 and nodes == no
+            assert cases.rel_err(y, yo) < Y_TOL
+            c_holder["checked"] = True
+            return y, nodes
+
+        seen["c"] = sysm.coupling(blk["jtot"], blk["block"])
+        assert seen["c"].n > 30
+        _, _, xs = _ityp6_block(g, sysm, blk, short_range=gpu_ldmd)
+        assert seen.get("checked")
+        _check_sigma(xs, blk)
