@@ -90,6 +90,21 @@ int mgpu_mdprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
 int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
                 double *z, int *nodes, int *kfail);
 
+/* The same two calls in the Fortran calling convention, every argument by
+ * reference and no structures, for an ISO_C_BINDING interface block with
+ * plain arrays (molscat_b200/fortran/mdprop_gpu.f, the replacement for
+ * source_code/mdprop.f and ldprop.f, binds these).  The arguments are the
+ * fields of mgpu_coupling / mgpu_grid, then Y (in/out), ERED, NODES, the
+ * failing step and *istat = MGPU_OK or the status mgpu_mdprop returns. */
+void mgpu_mdprop_f(const int *n, const int *nham, const int *nvlblk, const int *ivlfl, const int *nconst,
+                   const int *nrsq, const double *conlen, double *y, const double *vl, const int *iv,
+                   const double *eint, const double *cent, const int *nstep, const double *dr, const double *rtab,
+                   const double *ptab, const double *ered, int *nodes, int *kfail, int *istat);
+void mgpu_ldprop_f(const int *n, const int *nham, const int *nvlblk, const int *ivlfl, const int *nconst,
+                   const int *nrsq, const double *conlen, double *z, const double *vl, const int *iv,
+                   const double *eint, const double *cent, const int *nstep, const double *dr, const double *rtab,
+                   const double *ptab, const double *ered, int *nodes, int *kfail, int *istat);
+
 /* ---- batched propagation plans -----------------------------------------
  * A plan holds many systems and many jobs (one job = one propagation of a
  * system at one ERED) resident on the device.  For LDMD the energy

@@ -48,7 +48,7 @@ EXPORTS = (
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
     "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
     "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
-    "mgpu_plan_run_host_smatrix", "mgpu_probe_pivot_reciprocal",
+    "mgpu_plan_run_host_smatrix", "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
 )
 
 _lib = None

@@ -1848,6 +1848,59 @@ int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered, double 
     return single(MGPU_PROP_LDJ, c, g, ered, z, nodes, kfail);
 }
 
+// Fortran calling convention: every argument by reference, no structures.
+static void single_f(int iprop, const int *n, const int *nham, const int *nvlblk, const int *ivlfl,
+                     const int *nconst, const int *nrsq, const double *conlen, double *y, const double *vl,
+                     const int *iv, const double *eint, const double *cent, const int *nstep, const double *dr,
+                     const double *rtab, const double *ptab, const double *ered, int *nodes, int *kfail,
+                     int *istat)
+{
+    if (!istat) return;
+    if (!n || !nham || !nvlblk || !ivlfl || !nconst || !nrsq || !conlen || !nstep || !dr || !ered || !nodes ||
+        !kfail) {
+        *istat = set_err(MGPU_ERR_ARG, "null argument");
+        return;
+    }
+    mgpu_coupling c;
+    c.n = *n;
+    c.nham = *nham;
+    c.nvlblk = *nvlblk;
+    c.ivlfl = *ivlfl;
+    c.nconst = *nconst;
+    c.nrsq = *nrsq;
+    c.conlen = *conlen;
+    c.vl = vl;
+    c.iv = iv;
+    c.eint = eint;
+    c.cent = cent;
+    mgpu_grid g;
+    g.nstep = *nstep;
+    g.dr = *dr;
+    g.rtab = rtab;
+    g.ptab = ptab;
+    *nodes = 0;
+    *kfail = 0;
+    *istat = single(iprop, &c, &g, *ered, y, nodes, kfail);
+}
+
+void mgpu_mdprop_f(const int *n, const int *nham, const int *nvlblk, const int *ivlfl, const int *nconst,
+                   const int *nrsq, const double *conlen, double *y, const double *vl, const int *iv,
+                   const double *eint, const double *cent, const int *nstep, const double *dr, const double *rtab,
+                   const double *ptab, const double *ered, int *nodes, int *kfail, int *istat)
+{
+    single_f(MGPU_PROP_LDMD, n, nham, nvlblk, ivlfl, nconst, nrsq, conlen, y, vl, iv, eint, cent, nstep, dr, rtab,
+             ptab, ered, nodes, kfail, istat);
+}
+
+void mgpu_ldprop_f(const int *n, const int *nham, const int *nvlblk, const int *ivlfl, const int *nconst,
+                   const int *nrsq, const double *conlen, double *z, const double *vl, const int *iv,
+                   const double *eint, const double *cent, const int *nstep, const double *dr, const double *rtab,
+                   const double *ptab, const double *ered, int *nodes, int *kfail, int *istat)
+{
+    single_f(MGPU_PROP_LDJ, n, nham, nvlblk, ivlfl, nconst, nrsq, conlen, z, vl, iv, eint, cent, nstep, dr, rtab,
+             ptab, ered, nodes, kfail, istat);
+}
+
 }  // extern "C"
 
 // ===========================================================================
