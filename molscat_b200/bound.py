@@ -16,6 +16,7 @@ N symmetric eigenvalue count on the host (the propagation is the cost).
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 from typing import Callable
 
@@ -134,6 +135,126 @@ def bisect_steps(count: Callable, lo: float, hi: float, c_lo: int, c_hi: int, to
     return [(k, 0.5 * (a + b), a, b) for k, (a, b) in sorted(brackets.items())]
 
 
+def _zeroin(a: float, b: float, fa: float, fb: float, tol: float):
+    """Brent's zero finder (R. P. Brent, Algorithms for Minimization without
+    Derivatives, 1973, ch. 4) as a generator: yields the next abscissa,
+    receives f there, returns the root once the bracket is narrower than
+    about tol.  f(a) and f(b) must have opposite signs."""
+    eps = 2.220446049250313e-16
+    c, fc = a, fa
+    d = e = b - a
+    while True:
+        if fb * fc > 0.0:
+            c, fc = a, fa
+            d = e = b - a
+        if abs(fc) < abs(fb):
+            a, b, c = b, c, b
+            fa, fb, fc = fb, fc, fb
+        tol1 = 2.0 * eps * abs(b) + 0.5 * tol
+        xm = 0.5 * (c - b)
+        if abs(xm) <= tol1 or fb == 0.0:
+            return b
+        if abs(e) >= tol1 and abs(fa) > abs(fb):
+            s = fb / fa
+            if a == c:  # secant
+                p = 2.0 * xm * s
+                q = 1.0 - s
+            else:  # inverse quadratic interpolation
+                q = fa / fc
+                r = fb / fc
+                p = s * (2.0 * xm * q * (q - r) - (b - a) * (r - 1.0))
+                q = (q - 1.0) * (r - 1.0) * (s - 1.0)
+            if p > 0.0:
+                q = -q
+            p = abs(p)
+            if 2.0 * p < min(3.0 * xm * q - abs(tol1 * q), abs(e * q)):
+                e, d = d, p / q
+            else:
+                d = e = xm
+        else:
+            d = e = xm
+        a, fa = b, fb
+        b = b + d if abs(d) > tol1 else b + math.copysign(tol1, xm)
+        fb = yield b
+
+
+def converge_steps(evaluate: Callable, lo: float, hi: float, tol: float, coarse: float,
+                   max_rounds: int = 200):
+    """BOUND's search with its converging step (bd.driver.f:993-1215):
+    every step of a monotone count between lo and hi is bracketed by
+    bisection until only its own step lies inside, at most `coarse` wide,
+    and the matching eigenvalue of smallest magnitude has opposite signs at
+    the two ends; then that eigenvalue's zero is found by Brent's method to
+    `tol` (the reference's VWDB step, bd.driver.f:1139-1215).  Every live
+    bracket's next trial point goes into one call of evaluate(xs) ->
+    (counts, smallest matching eigenvalues) per round.
+
+    Returns ([(k, x, lo, hi)], rounds): the step between counts k and k+1 at
+    x, within its final bracket, and the number of evaluate calls."""
+    c, g = evaluate(np.array([lo, hi]))
+    c_lo, c_hi = int(c[0]), int(c[1])
+    inc = c_hi >= c_lo
+    rounds = 1
+    br = {k: dict(lo=lo, hi=hi, clo=c_lo, chi=c_hi, glo=float(g[0]), ghi=float(g[1]))
+          for k in range(min(c_lo, c_hi), max(c_lo, c_hi))}
+    # count at the low end of step k's bracket is k (increasing) or k+1
+    want_lo = (lambda k: k) if inc else (lambda k: k + 1)
+    want_hi = (lambda k: k + 1) if inc else (lambda k: k)
+    done = {}
+    gens = {}
+    pending = {}
+
+    def ready(k, b):
+        if b["clo"] != want_lo(k) or b["chi"] != want_hi(k) or b["hi"] - b["lo"] > coarse:
+            return False
+        return b["glo"] * b["ghi"] < 0.0
+
+    while len(done) < len(br) and rounds < max_rounds:
+        xs, who = [], []
+        for k, b in br.items():
+            if k in done:
+                continue
+            if k in gens:
+                xs.append(pending[k])
+                who.append((k, "brent"))
+            elif ready(k, b):
+                gen = _zeroin(b["lo"], b["hi"], b["glo"], b["ghi"], tol)
+                gens[k] = gen
+                pending[k] = next(gen)
+                xs.append(pending[k])
+                who.append((k, "brent"))
+            elif b["hi"] - b["lo"] <= tol:
+                done[k] = 0.5 * (b["lo"] + b["hi"])
+            else:
+                xs.append(0.5 * (b["lo"] + b["hi"]))
+                who.append((k, "bisect"))
+        if not xs:
+            break
+        cnt, eig = evaluate(np.array(xs))
+        rounds += 1
+        for (k, how), x, cn, gv in zip(who, xs, cnt, eig):
+            cn, gv = int(cn), float(gv)
+            # every bisection point tightens the brackets it falls in
+            for kk, b in br.items():
+                if kk in done or kk in gens or not (b["lo"] < x < b["hi"]):
+                    continue
+                below = (cn <= kk) if inc else (cn > kk)
+                if below:
+                    b.update(lo=x, clo=cn, glo=gv)
+                else:
+                    b.update(hi=x, chi=cn, ghi=gv)
+            if how == "brent":
+                try:
+                    pending[k] = gens[k].send(gv)
+                except StopIteration as stop:
+                    done[k] = stop.value
+                    del gens[k]
+    for k in br:
+        if k not in done:
+            done[k] = pending.get(k, 0.5 * (br[k]["lo"] + br[k]["hi"]))
+    return [(k, done[k], br[k]["lo"], br[k]["hi"]) for k in sorted(br)], rounds
+
+
 def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_rounds: int = 200,
                 counter: Callable | None = None) -> list:
     """Every state with EMIN < E < EMAX (reduced energies), bisected until its
@@ -144,3 +265,15 @@ def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_roun
     count = counter or (lambda b, e: node_counts(b, e)[0])
     c0, c1 = (int(x) for x in count(bp, [emin, emax]))
     return bisect_steps(lambda xs: count(bp, xs), emin, emax, c0, c1, tol, max_rounds)
+
+
+def find_states_converged(bp: BoundProblem, emin: float, emax: float, tol: float, coarse: float = math.inf,
+                          max_rounds: int = 200, evaluate: Callable | None = None):
+    """Every state with EMIN < E < EMAX (reduced energies) by bisection to a
+    bracket at most `coarse` wide holding that state alone, then Brent's
+    method on the smallest matching eigenvalue to `tol` (converge_steps).
+    Returns ([(node count k, energy, lo, hi)], propagation rounds).
+    `evaluate(bp, ereds) -> (counts, smallest matching eigenvalues)` defaults
+    to the GPU (node_counts)."""
+    ev = evaluate or (lambda b, e: (lambda r: (r[0], r[4]))(node_counts(b, e)))
+    return converge_steps(lambda xs: ev(bp, xs), emin, emax, tol, coarse, max_rounds)

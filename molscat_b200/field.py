@@ -17,12 +17,13 @@ segments of all fields together), so one GPU launch set serves all states.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 from typing import Callable
 
 import numpy as np
 
-from .bound import adiabatic_wkb_y, bisect_steps
+from .bound import adiabatic_wkb_y, bisect_steps, converge_steps
 from .propagators import Coupling, Plan, Segment
 
 
@@ -46,8 +47,9 @@ class FieldProblem:
 
 
 def field_node_counts(fp: FieldProblem, fields) -> tuple:
-    """(counts, NODES_out, NODES_in, matching counts) at every field, all
-    fields' propagations in one plan."""
+    """(counts, NODES_out, NODES_in, matching counts, smallest-magnitude
+    matching eigenvalues) at every field, all fields' propagations in one
+    plan."""
     fields = np.asarray(fields, dtype=np.float64)
     m = fields.size
     cs = [fp.coupling_at(float(f)) for f in fields]
@@ -60,11 +62,15 @@ def field_node_counts(fp: FieldProblem, fields) -> tuple:
             j = int(np.nonzero(status)[0][0])
             raise RuntimeError(f"propagation failed at F={fields[j % m]} (status {int(status[j])}, "
                                f"step {int(kfail[j])})")
-        nmatch = np.array([int(np.sum(np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k)) <= 0.0))
-                           for k in range(m)], dtype=np.int64)
+        nmatch = np.zeros(m, dtype=np.int64)
+        eigmin = np.zeros(m)
+        for k in range(m):
+            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k))
+            nmatch[k] = int(np.sum(ev <= 0.0))
+            eigmin[k] = ev[np.argmin(np.abs(ev))]
         n_out = nodes[:m].astype(np.int64)
         n_in = nodes[m:].astype(np.int64)
-        return n_out + n_in + nmatch, n_out, n_in, nmatch
+        return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
     finally:
         plan.close()
 
@@ -79,3 +85,15 @@ def find_fields(fp: FieldProblem, fmin: float, fmax: float, tol: float, max_roun
     count = counter or (lambda p, f: field_node_counts(p, f)[0])
     c0, c1 = (int(x) for x in count(fp, [fmin, fmax]))
     return bisect_steps(lambda xs: count(fp, xs), fmin, fmax, c0, c1, tol, max_rounds)
+
+
+def find_fields_converged(fp: FieldProblem, fmin: float, fmax: float, tol: float, coarse: float = math.inf,
+                          max_rounds: int = 200, evaluate: Callable | None = None):
+    """FIELD's search with its converging step (fld.driver.f:1102-1217):
+    bisection on the field until each crossing sits alone in its bracket with
+    the matching eigenvalue changing sign, then Brent's method on that
+    eigenvalue to `tol` (bound.converge_steps).  Returns ([(k, field, lo,
+    hi)], propagation rounds).  `evaluate(fp, fields) -> (counts, smallest
+    matching eigenvalues)` defaults to the GPU."""
+    ev = evaluate or (lambda p, f: (lambda r: (r[0], r[4]))(field_node_counts(p, f)))
+    return converge_steps(lambda xs: ev(fp, xs), fmin, fmax, tol, coarse, max_rounds)

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import cases
-from molscat_b200.bound import BoundProblem, adiabatic_wkb_y, find_states
+from molscat_b200.bound import BoundProblem, adiabatic_wkb_y, find_states, find_states_converged
 from molscat_b200.propagators import Coupling, Segment, radial_grid
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -49,6 +49,23 @@ def oracle_counts(bp, ereds):
         assert st == 0 and st2 == 0
         out.append(no + ni + int(np.sum(np.linalg.eigvalsh(yo - yi) <= 0.0)))
     return np.array(out)
+
+
+def oracle_eval(bp, ereds):
+    """(counts, smallest-magnitude matching eigenvalue) with the oracle."""
+    from oracle import oracle as O
+    oc = cases.to_oracle(bp.coupling)
+    cnt, eig = [], []
+    for e in ereds:
+        yo, no, st, _ = O.mdprop(oc, bp.seg_out.rtab, bp.seg_out.ptab, bp.seg_out.nstep, bp.seg_out.dr, e,
+                                 bp.y_out0(float(e)))
+        yi, ni, st2, _ = O.mdprop(oc, bp.seg_in.rtab, bp.seg_in.ptab, bp.seg_in.nstep, bp.seg_in.dr, e,
+                                  bp.y_in0(float(e)))
+        assert st == 0 and st2 == 0
+        ev = np.linalg.eigvalsh(yo - yi)
+        cnt.append(no + ni + int(np.sum(ev <= 0.0)))
+        eig.append(float(ev[np.argmin(np.abs(ev))]))
+    return np.array(cnt), np.array(eig)
 
 
 def _states(bp, sysm, g, counter=None):
@@ -111,3 +128,60 @@ def test_bisection_brackets_every_state_with_a_counting_stub():
         assert abs(e - lev) <= tol
     # every round puts all unresolved states' trial energies into one batch
     assert calls[0] == 2 and max(calls[1:]) <= len(inside)
+
+
+def _converged(bp, sysm, g, evaluate=None):
+    s = g["system"]
+    res, rounds = find_states_converged(bp, s["emin_cm"] * sysm.cm2ru, s["emax_cm"] * sysm.cm2ru,
+                                        TOL_CM * sysm.cm2ru, evaluate=evaluate)
+    return [(k + 1, e / sysm.cm2ru) for k, e, _, _ in res], rounds
+
+
+def test_converged_search_with_oracle_matches_reference(basic1):
+    """Bisection until each state sits alone in its bracket with the matching
+    eigenvalue changing sign, then Brent on that eigenvalue (the VWDB step of
+    bd.driver.f:1139-1215): the reference's energies in far fewer
+    propagation rounds than bisecting to the same width."""
+    g, sysm, bp = basic1
+    got, rounds = _converged(bp, sysm, g, evaluate=oracle_eval)
+    want = [(st["state"], st["energy_cm"]) for st in g["states"]]
+    assert [k for k, _ in got] == [k for k, _ in want]
+    for (_, e), (_, w) in zip(got, want):
+        assert abs(e - w) < REF_TOL_CM, (e, w)
+    calls = []
+    _states(bp, sysm, g, counter=lambda b, e: (calls.append(1), oracle_counts(b, e))[1])
+    assert rounds < len(calls) / 2, (rounds, len(calls))
+
+
+def test_converged_search_with_a_stub():
+    """The search logic alone: counts and a matching eigenvalue with known
+    zeros stand in for the propagations."""
+    levels = np.array([-7.25, -3.5, -3.4999, -1.0, 0.75])
+    rounds_seen = []
+
+    def stub(bp, ereds):
+        e = np.asarray(ereds, dtype=np.float64)
+        cnt = np.searchsorted(levels, e, side="left")
+        near = levels[np.argmin(np.abs(e[:, None] - levels[None, :]), axis=1)]
+        rounds_seen.append(e.size)
+        return cnt, -(e - near) * (1.0 + 0.3 * (e - near))  # positive below a level, negative above
+
+    found, rounds = find_states_converged(None, -5.0, 1.0, 1e-12, evaluate=stub)
+    inside = levels[(levels > -5.0) & (levels < 1.0)]
+    assert [k for k, *_ in found] == [1, 2, 3, 4]
+    for (k, e, lo, hi), lev in zip(found, inside):
+        assert abs(e - lev) <= 1e-11
+    assert rounds == len(rounds_seen) and rounds < 60
+
+
+@pytest.mark.gpu
+def test_gpu_converged_search_equals_oracle(basic1):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    g, sysm, bp = basic1
+    got, rounds = _converged(bp, sysm, g)
+    ora, _ = _converged(bp, sysm, g, evaluate=oracle_eval)
+    assert [k for k, _ in got] == [k for k, _ in ora]
+    for (_, e), (_, o) in zip(got, ora):
+        assert abs(e - o) <= 1e-9 * abs(o), (e, o)

@@ -13,8 +13,8 @@ import numpy as np
 import pytest
 
 from molscat_b200.bound import bisect_steps
-from molscat_b200.field import FieldProblem, field_node_counts, find_fields
-from test_bound import REF_TOL_CM, TOL_CM, basic1, oracle_counts  # noqa: F401  (fixture)
+from molscat_b200.field import FieldProblem, field_node_counts, find_fields, find_fields_converged
+from test_bound import REF_TOL_CM, TOL_CM, basic1, oracle_counts, oracle_eval  # noqa: F401  (fixture)
 
 E_CM = -3.0
 
@@ -84,3 +84,40 @@ def test_gpu_field_counts_equal_oracle(basic1):
     # so equal counts at every midpoint give identical fields
     ora = sorted(f for _, f, _, _ in find_fields(fp, fmin, fmax, TOL_CM, counter=oracle_field_counts))
     assert got == ora
+
+
+def oracle_field_eval(fp, fields):
+    from molscat_b200.bound import BoundProblem
+    cnt, eig = [], []
+    for f in fields:
+        c = fp.coupling_at(float(f))
+        bp = BoundProblem(c, fp.seg_out, fp.seg_in, fp.prop,
+                          y_out0=lambda e, c=c: fp.y_out0(c), y_in0=lambda e, c=c: fp.y_in0(c))
+        a, b = oracle_eval(bp, [fp.ered])
+        cnt.append(int(a[0]))
+        eig.append(float(b[0]))
+    return np.array(cnt), np.array(eig)
+
+
+@pytest.mark.parametrize("sign", [1, -1])
+def test_oracle_converged_fields_match_reference_energies(basic1, sign):
+    fp, (fmin, fmax), want = field_problem(basic1, sign)
+    found, rounds = find_fields_converged(fp, fmin, fmax, TOL_CM, evaluate=oracle_field_eval)
+    got = sorted(f for _, f, _, _ in found)
+    assert len(got) == len(want)
+    for f, w in zip(got, want):
+        assert abs(f - w) < REF_TOL_CM, (f, w)
+    assert rounds < 25
+
+
+@pytest.mark.gpu
+def test_gpu_converged_fields_equal_oracle(basic1):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    fp, (fmin, fmax), want = field_problem(basic1, 1)
+    got = sorted(f for _, f, _, _ in find_fields_converged(fp, fmin, fmax, TOL_CM)[0])
+    ora = sorted(f for _, f, _, _ in find_fields_converged(fp, fmin, fmax, TOL_CM, evaluate=oracle_field_eval)[0])
+    assert len(got) == len(want) == len(ora)
+    for f, o in zip(got, ora):
+        assert abs(f - o) <= 1e-9 * abs(o), (f, o)
