@@ -12,8 +12,10 @@ published dataset for this path).
 
 Metric: channel^3*steps/s = sum over propagations of N^3*NSTEP, divided by the
 device time of the step (the whole job; max over ranks).  solves/s and the
-counted FP64 rate ride along.  Multi-GPU: every rank runs its own batch
-(different energy draw); no collective on the data path ("weak").
+counted FP64 rate ride along.  Multi-GPU (weak scaling): N x 512 energies,
+cut into units of one block and 512 energies spread over the ranks by LPT
+(molscat_b200/sharding.py), so each GPU holds about the single-GPU
+workload; no collective on the data path, time = max over ranks.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 """
@@ -550,7 +552,11 @@ def main():
     tuned = autotune.apply(tpath) if os.path.exists(tpath) else 0
 
     t_setup = time.perf_counter()
-    wl = S.batched_workload(n_energies=args.energies, jmax=args.jmax, seed=20261203 + rank)
+    if world > 1:
+        # weak scaling through the sharding path: world x 512 energies, LPT units of one block and 512 energies
+        wl = S.batched_workload_shard(rank, world, n_energies=args.energies, jmax=args.jmax)
+    else:
+        wl = S.batched_workload(n_energies=args.energies, jmax=args.jmax)
     plan = Plan("LDMD", wl.systems, wl.segments, wl.job_sys, wl.job_ered)
     y0_host = plan.pack(wl.job_y0)
     t_setup = time.perf_counter() - t_setup
@@ -686,7 +692,8 @@ def main():
                        "systems": len(wl.systems), "propagations_per_gpu": njobs,
                        "l2": "inputs larger than L2 (2HQ(C) tables %.1f GB)" % (plan.flops_prep and
                                                                                  sum(16 * (((s.n + 3) // 4) * ((s.n + 3) // 4 + 1) // 2) * 8 * 4000 for s in wl.systems) / 1e9),
-                       "parallelism": "independent batches per GPU (no collective)" if world > 1 else "1 GPU",
+                       "parallelism": ("LPT shards of (block, 512 energies) units over %d GPUs, no collective on the "
+                                       "data path" % world) if world > 1 else "1 GPU",
                        "tuning": f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"},
             "solves_per_s": jobs_all / (ms * 1e-3),
             "flops_counted_per_s": plan.flops * world / (ms * 1e-3),

@@ -81,3 +81,23 @@ def run_sharded(wl: Workload, rank: int, world: int, run: Callable, group=None) 
     for p in parts:
         out.update(p)
     return out
+
+
+def gpu_run(prop: str = "LDMD") -> Callable:
+    """The per-rank `run` of run_sharded on this process's current GPU: all
+    of the shard's systems and jobs in one batched plan (the energies of a
+    block share its 2HQ(C) table), Y in and out through host buffers."""
+    def run(wl: Workload):
+        from .propagators import Plan
+        plan = Plan(prop, wl.systems, wl.segments, wl.job_sys, wl.job_ered)
+        try:
+            ybuf, nodes, status, _ = plan.run_host(plan.pack(wl.job_y0))
+            return [plan.unpack(ybuf, j).copy() for j in range(wl.njobs)], nodes, status
+        finally:
+            plan.close()
+    return run
+
+
+def rank_units(costs, rank: int, world: int) -> np.ndarray:
+    """The units (by index into `costs`) this rank propagates under LPT."""
+    return lpt_partition(costs, world)[rank]

@@ -235,6 +235,44 @@ def batched_workload(n_energies: int = 512, jmax: int = 80, seed: int = 20261203
                        nstep=nstep)
 
 
+def batched_workload_shard(rank: int, world: int, n_energies: int = 512, jmax: int = 80,
+                           seed: int = 20261203, nstep: int = ROTOR_NSTEP) -> Workload:
+    """This rank's part of the multi-GPU batched workload (weak scaling): the
+    JTOT = 0..jmax x 2 parities blocks at world * n_energies seeded energies,
+    cut into units of one block and n_energies energies, the units spread
+    over ranks by LPT on N^3 * NSTEP * energies (sharding.lpt_partition), so
+    every rank holds about one GPU's worth of the single-GPU workload and a
+    block's energies on a rank share its 2HQ(C) table."""
+    from .sharding import rank_units
+    sysm = rotor_system()
+    e_all = batched_energies(n_energies * world, seed)
+    units = [(jt, b, k) for jt in range(jmax + 1) for b in (1, 2) if sysm.channels(jt, b) for k in range(world)]
+    costs = [len(sysm.channels(jt, b)) ** 3 * float(nstep) * n_energies for jt, b, _ in units]
+    mine = [units[i] for i in rank_units(costs, rank, world)]
+    rmin, rmax = ROTOR_RMIN_A / sysm.rm, ROTOR_RMAX_A / sysm.rm
+    dr = (rmax - rmin) / nstep
+    seg = None
+    systems, segments, labels, job_sys, job_ered, job_y0 = [], [], [], [], [], []
+    sys_of = {}
+    for jt, b, k in mine:
+        if (jt, b) not in sys_of:
+            c = sysm.coupling(jt, b)
+            if seg is None:
+                seg = Segment.build(rmin, dr, nstep, sysm.pvec, c.nham)
+            sys_of[(jt, b)] = len(systems)
+            systems.append(c)
+            segments.append(seg)
+            labels.append((jt, b))
+        s = sys_of[(jt, b)]
+        for e in e_all[k * n_energies:(k + 1) * n_energies]:
+            ered = e * sysm.cm2ru
+            job_sys.append(s)
+            job_ered.append(ered)
+            job_y0.append(wkb_initial_y(systems[s], seg.ptab[0], seg.rtab[0], ered))
+    return Workload(f"rotor JTOT=0..{jmax} x 2 parities x {n_energies * world} energies, rank {rank}/{world}",
+                    systems, segments, np.array(job_sys, dtype=np.int32), np.array(job_ered), job_y0, labels)
+
+
 def synthetic_system(n: int, nstep: int = 3000, seed: int = 0, nham: int = 6):
     """A dense coupled-channel system of exactly N channels for timing large
     and mixed N: NHAM Lennard-Jones 12-6 radial terms with seeded amplitudes

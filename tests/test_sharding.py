@@ -109,3 +109,51 @@ def test_two_ranks_gloo_equal_single_process(tmp_path):
             assert st == sts == 0
             assert nd == nds
             assert np.array_equal(y, ys)
+
+
+def _gpu_worker(rank, world, port, out_dir):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    torch.cuda.set_device(0)  # both ranks share the one GPU: their kernels never wait on each other
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    try:
+        wl = small_workload()
+        res = sharding.run_sharded(wl, rank, world, sharding.gpu_run())
+        with open(os.path.join(out_dir, f"gpu_rank{rank}.pkl"), "wb") as f:
+            pickle.dump(res, f)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_sharded_cuda_path_equals_oracle_and_single_process(tmp_path):
+    """The CUDA library as each rank's propagator: world size 1 against the
+    oracle (NODES exact, Y within 5e-8), then two gloo ranks (one GPU, each
+    its own process and plan) gathering results equal to world size 1's bit
+    for bit."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from molscat_b200.build import build
+    build()
+    wl = small_workload()
+    one = sharding.run_sharded(wl, 0, 1, sharding.gpu_run())
+    ora = sharding.run_sharded(wl, 0, 1, oracle_run)
+    assert sorted(one) == list(range(wl.njobs))
+    for j, (y, nd, st) in one.items():
+        yo, ndo, sto = ora[j]
+        assert st == sto == 0 and nd == ndo
+        assert cases.rel_err(y, yo) < 5e-8
+    import torch.multiprocessing as mp
+    world = 2
+    mp.start_processes(_gpu_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        with open(tmp_path / f"gpu_rank{r}.pkl", "rb") as f:
+            res = pickle.load(f)
+        assert sorted(res) == list(range(wl.njobs))
+        for j, (y, nd, st) in res.items():
+            assert st == one[j][2] and nd == one[j][1]
+            assert np.array_equal(y, one[j][0])
