@@ -50,6 +50,8 @@ extern "C" {
 #define MGPU_ERR_UNSUPPORTED 5 /* N above the largest compiled bucket */
 #define MGPU_ERR_NOMEM 6       /* device allocation failed */
 #define MGPU_ERR_TIMEOUT 7     /* a bounded in-kernel wait (TMA copy) expired */
+#define MGPU_ERR_CANCELLED 8   /* the host cancelled the plan (mgpu_plan_cancel) */
+#define MGPU_ERR_DEADLINE 9    /* a step kernel ran past the plan's time limit (mgpu_plan_set_time_limit) */
 
 /* propagator ids (IPROP values of scctrl.f:170-196) */
 #define MGPU_PROP_LDJ 5  /* Johnson log-derivative, LDPROP */
@@ -163,6 +165,27 @@ int mgpu_plan_smatrix_device(mgpu_plan *plan, const double *y_dev, double *sr_de
 /* host buffers: initial Y in, S matrices and NODES / status / failing step out */
 int mgpu_plan_run_host_smatrix(mgpu_plan *plan, const double *y, double *sr, double *si, int *nodes,
                                int *status, int *kfail);
+
+/* Stopping a plan's runs from the host.  The step kernels of the one-warp,
+ * one-CTA and 4x4-tile families (N <= 200; LDPROP <= 128) poll the plan's
+ * controls every 128 steps (steps 1, 129, 257, ...) and a job that sees a
+ * stop leaves its step loop with the status and the step recorded, as after
+ * a failed inversion; the large-N kernels run their steps to the end.
+ * mgpu_plan_cancel(plan, 1): runs in progress and later runs stop with
+ *   MGPU_ERR_CANCELLED (callable from any host thread while a run is in
+ *   flight: the controls live in mapped host memory); (plan, 0) clears it.
+ * mgpu_plan_set_time_limit(plan, s): a step kernel that has run longer than s
+ *   seconds (the device's global timer, from that kernel's start) stops its
+ *   jobs with MGPU_ERR_DEADLINE; 0 removes the limit. */
+int mgpu_plan_cancel(mgpu_plan *plan, int on);
+int mgpu_plan_set_time_limit(mgpu_plan *plan, double seconds);
+
+/* For tests of the timeout path: the iteration limit of the one-warp step
+ * kernels' wait for each step's 2HQ(C) copy (limit >= 0; 0 gives up at
+ * once, so every job reports MGPU_ERR_TIMEOUT at step 1; -1 restores the
+ * default).  The waits that let copies in flight land before an early exit
+ * keep the full limit.  Process-wide, current device. */
+int mgpu_set_step_wait_limit(int limit);
 
 /* The number of kernel launches one run of the plan makes. */
 int mgpu_plan_launches(const mgpu_plan *plan);

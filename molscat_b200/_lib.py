@@ -18,6 +18,8 @@ MGPU_ERR_CUDA = 4
 MGPU_ERR_UNSUPPORTED = 5
 MGPU_ERR_NOMEM = 6
 MGPU_ERR_TIMEOUT = 7
+MGPU_ERR_CANCELLED = 8
+MGPU_ERR_DEADLINE = 9
 
 MGPU_PROP_LDJ = 5
 MGPU_PROP_LDMD = 6
@@ -49,6 +51,7 @@ EXPORTS = (
     "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
     "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
     "mgpu_plan_run_host_smatrix", "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
+    "mgpu_plan_cancel", "mgpu_plan_set_time_limit", "mgpu_set_step_wait_limit",
 )
 
 _lib = None
@@ -86,6 +89,9 @@ def load(path: str | None = None):
     L.mgpu_plan_flops_phase.restype = ctypes.c_double
     L.mgpu_probe_fp64_fma.argtypes = [vp, ctypes.c_int, vp, _dp]
     L.mgpu_probe_pivot_reciprocal.argtypes = [vp, vp, ctypes.c_int, vp]
+    L.mgpu_plan_cancel.argtypes = [vp, ctypes.c_int]
+    L.mgpu_plan_set_time_limit.argtypes = [vp, ctypes.c_double]
+    L.mgpu_set_step_wait_limit.argtypes = [ctypes.c_int]
     L.mgpu_mdprop_noalloc.argtypes = [pc, pg, ctypes.c_int, vp, vp, vp, vp, vp, vp]
     L.mgpu_status_string.argtypes = [ctypes.c_int]
     L.mgpu_status_string.restype = ctypes.c_char_p

@@ -272,6 +272,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
     extern __shared__ __align__(16) double sm[];
     __shared__ TileRC tab[C::NTL];
     __shared__ int cf[2];
+    __shared__ int s_stop;
     __shared__ SysDev s_sys;
     const JobDev job = jobs[blockIdx.x];
     if (threadIdx.x == 0) s_sys = systems[job.sys];
@@ -315,7 +316,18 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
     }
     __syncthreads();
     int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
     for (int k = 1; k <= nstep; ++k) {
+        if (stop_poll_step(k)) {  // host cancel / time limit: thread 0's reading for the CTA
+            if (tid == 0) s_stop = stop_requested(S.ctl, t0);
+            __syncthreads();  // the next write comes kStopPoll steps (and their barriers) later
+            const int stop = s_stop;
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         // reference-potential solutions (mdprop.f:143-164)
         for (int i = tid; i < n; i += C::NTHR) {
             const double wref = wf::w_diag_frag<NT>(S, i, 2 * k - 1, ered);
@@ -398,6 +410,7 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
     extern __shared__ __align__(16) double sm[];
     __shared__ TileRC tab[C::NTL];
     __shared__ int cf[2];
+    __shared__ int s_stop;
     __shared__ SysDev s_sys;
     const JobDev job = jobs[blockIdx.x];
     if (threadIdx.x == 0) s_sys = systems[job.sys];
@@ -426,7 +439,18 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
     }
     __syncthreads();
     int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
     for (int k = 1; k <= S.nstep; ++k) {
+        if (stop_poll_step(k)) {
+            if (tid == 0) s_stop = stop_requested(S.ctl, t0);
+            __syncthreads();  // the next write comes kStopPoll steps (and their barriers) later
+            const int stop = s_stop;
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         const double *P = S.ptab + (size_t)(2 * k - 1) * S.nham;
         for (int x = tid; x < C::TD; x += C::NTHR) {
             int i, j;

@@ -265,7 +265,18 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     const int r = lane >> 2, q = lane & 3;
     int nodes = 0, status = MGPU_OK, kfail = 0;
     int issued = 1, consumed = 0;
+    const unsigned long long t0 = global_ns();
+    const uint32_t wait_limit = g_step_wait_limit;
     for (int k = 1; k <= nstep; ++k) {
+        if (stop_poll_step(k)) {  // host cancel / time limit, lane 0's reading for the warp
+            int stop = lane == 0 ? stop_requested(S.ctl, t0) : MGPU_OK;
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         // reference-potential solutions in the sector (mdprop.f:143-164)
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
@@ -289,7 +300,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
             kfail = k;
             break;
         }
-        const bool landed = mbar_wait_bounded(bar, (k - 1) & 1);
+        const bool landed = mbar_wait_bounded(bar, (k - 1) & 1, wait_limit);
         if (__any_sync(0xffffffffu, !landed)) {
             status = MGPU_ERR_TIMEOUT;
             kfail = k;
@@ -404,7 +415,17 @@ ldj_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
                 z[tix(I, J)][s] = h * z[tix(I, J)][s] + d1 * u[tix(I, J)][s] + (dg ? 1.0 : 0.0);  // ldprop.f:46-51
             }
     int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
     for (int k = 1; k <= S.nstep; ++k) {
+        if (stop_poll_step(k)) {
+            int stop = lane == 0 ? stop_requested(S.ctl, t0) : MGPU_OK;
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         w_frag<NT>(S, lane, 2 * k - 1, ered, true, u);
 #pragma unroll
         for (int I = 0; I < NT; ++I)

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -43,6 +44,7 @@ struct SysDev {
     const double *ptab; // [2*nstep+1][nham]
     double *q;          // LDMD: [nstep][T*T][ntiles] 2HQ(C_k)
     int *prep;          // LDMD: [0] negative pivots of all U inversions (NSAVE), [1] status, [2] kfail
+    const volatile long long *ctl;  // plan's stop controls (mapped host memory) or null: stop_requested
 };
 
 struct JobDev {
@@ -271,6 +273,7 @@ ldmd_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ 
     __shared__ __align__(16) double vb[2 * G::VS];
     __shared__ double s_y14[2][NPAD], s_y14b[2][NPAD], s_y23[2][NPAD];
     __shared__ __align__(8) uint64_t qbar[2];
+    __shared__ int s_stop;
     __shared__ SysDev s_sys;
     const JobDev job = jobs[blockIdx.x];
     if (threadIdx.x == 0) s_sys = systems[job.sys];
@@ -338,7 +341,18 @@ ldmd_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ 
     int status = MGPU_OK, kfail = 0;
     int issued = 1;    // last step whose 2HQ(C) copy has been started
     int consumed = 0;  // last step whose copy has been waited for
+    const unsigned long long t0 = global_ns();
     for (int k = 1; k <= S.nstep; ++k) {
+        if (stop_poll_step(k)) {  // host cancel / time limit: thread 0's reading for the CTA
+            if (tid == 0) s_stop = stop_requested(S.ctl, t0);
+            __syncthreads();  // the next write comes kStopPoll steps (and their barriers) later
+            const int stop = s_stop;
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         const int sb = k & 1;
         if (tid == 0 && k + 1 <= S.nstep) {
             // buffer (k+1)&1 was last read in step k-1; every thread has passed
@@ -441,6 +455,7 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
     extern __shared__ __align__(16) double dsm[];
     __shared__ __align__(16) double vz[2 * G::VS];
     __shared__ __align__(16) double vu[2 * G::VS];
+    __shared__ int s_stop;
     __shared__ SysDev s_sys;
     const JobDev job = jobs[blockIdx.x];
     if (threadIdx.x == 0) s_sys = systems[job.sys];
@@ -478,7 +493,18 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
             }
     }
     int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
     for (int k = 1; k <= S.nstep; ++k) {
+        if (stop_poll_step(k)) {
+            if (tid == 0) s_stop = stop_requested(S.ctl, t0);
+            __syncthreads();
+            const int stop = s_stop;
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = k;
+                break;
+            }
+        }
         if (act) {
             w_tile<T>(S, vl, tid, I, J, 2 * k - 1, ered, true, u);
 #pragma unroll
@@ -981,6 +1007,9 @@ struct mgpu_plan {
     std::vector<BigStreams> bstreams;
     cudaStream_t own = nullptr;            // run_host's copies and launches
     cudaEvent_t ev_in = nullptr;
+    // stop controls the step kernels poll: [0] cancel, [1] time budget (ns), mapped host memory
+    volatile long long *ctl = nullptr;
+    const volatile long long *d_ctl = nullptr;
     // host staging for run_host
     double *d_y = nullptr;
     int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
@@ -1010,6 +1039,7 @@ struct mgpu_plan {
         if (d_kfail) cudaFree(d_kfail);
         if (d_sr) cudaFree(d_sr);
         if (d_si) cudaFree(d_si);
+        if (ctl) cudaFreeHost((void *)ctl);
     }
     template <class X>
     cudaError_t dalloc(X **p, size_t count)
@@ -1139,6 +1169,7 @@ static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, i
     d.rtab = drt;
     d.ptab = dpt;
     d.q = dq;
+    d.ctl = nullptr;
     return MGPU_OK;
 }
 
@@ -1378,6 +1409,32 @@ int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_
     return MGPU_OK;
 }
 
+int mgpu_plan_cancel(mgpu_plan *plan, int on)
+{
+    if (!plan || !plan->ctl) return set_err(MGPU_ERR_ARG, "null plan");
+    plan->ctl[0] = on ? 1 : 0;
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    return MGPU_OK;
+}
+
+int mgpu_plan_set_time_limit(mgpu_plan *plan, double seconds)
+{
+    if (!plan || !plan->ctl) return set_err(MGPU_ERR_ARG, "null plan");
+    if (!(seconds >= 0.0) || !std::isfinite(seconds)) return set_err(MGPU_ERR_ARG, "time limit must be >= 0");
+    const double ns = seconds * 1.0e9;
+    plan->ctl[1] = (seconds == 0.0) ? 0 : (ns < 1.0 ? 1 : (ns > 9.0e18 ? (long long)9e18 : (long long)ns));
+    std::atomic_thread_fence(std::memory_order_seq_cst);
+    return MGPU_OK;
+}
+
+int mgpu_set_step_wait_limit(int limit)
+{
+    const uint32_t v = limit < 0 ? kWaitLimit : (uint32_t)limit;
+    cudaError_t e = cudaMemcpyToSymbol(g_step_wait_limit, &v, sizeof v);
+    if (e != cudaSuccess) return set_err(MGPU_ERR_CUDA, "setting the step wait limit", e);
+    return MGPU_OK;
+}
+
 int mgpu_probe_pivot_reciprocal(const double *x_dev, double *r_dev, int n, void *stream)
 {
     if (!x_dev || !r_dev || n < 0) return set_err(MGPU_ERR_ARG, "probe arguments");
@@ -1401,6 +1458,8 @@ const char *mgpu_status_string(int s)
     case MGPU_ERR_UNSUPPORTED: return "unsupported size";
     case MGPU_ERR_NOMEM: return "device allocation failed";
     case MGPU_ERR_TIMEOUT: return "bounded wait for an asynchronous copy expired";
+    case MGPU_ERR_CANCELLED: return "cancelled by the host";
+    case MGPU_ERR_DEADLINE: return "time limit of a step kernel exceeded";
     default: return "unknown status";
     }
 }
@@ -1501,6 +1560,20 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         return set_err(MGPU_ERR_NOMEM, "allocating prep counters", e);
     }
     for (int s = 0; s < nsys; ++s) hs[s].prep = p->d_prep + 3 * s;
+    {
+        void *h = nullptr, *dptr = nullptr;
+        if ((e = cudaHostAlloc(&h, 2 * sizeof(long long), cudaHostAllocMapped)) ||
+            (e = cudaHostGetDevicePointer(&dptr, h, 0))) {
+            if (h) cudaFreeHost(h);
+            delete p;
+            return set_err(MGPU_ERR_NOMEM, "allocating the stop controls", e);
+        }
+        p->ctl = static_cast<volatile long long *>(h);
+        p->ctl[0] = 0;
+        p->ctl[1] = 0;
+        p->d_ctl = static_cast<const volatile long long *>(dptr);
+    }
+    for (int s = 0; s < nsys; ++s) hs[s].ctl = p->d_ctl;
     if ((e = upload(p, &p->d_sys, hs.data(), hs.size()))) {
         delete p;
         return set_err(MGPU_ERR_NOMEM, "uploading system descriptors", e);

@@ -298,11 +298,43 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
 // did not land within the limit (the caller reports a timeout status).
 constexpr uint32_t kWaitLimit = 1u << 22;
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit = kWaitLimit)
 {
-    for (uint32_t it = 0; it < kWaitLimit; ++it)
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_test(bar, parity)) return true;
     return false;
+}
+
+// Iteration limit of the one-warp kernels' per-step wait for the next
+// 2HQ(C) copy (kWaitLimit unless a test lowers it through
+// mgpu_set_step_wait_limit; the waits that drain copies before an early
+// exit always use kWaitLimit).
+__device__ uint32_t g_step_wait_limit = kWaitLimit;
+
+// A stop the host asks for, polled by the step kernels every kStopPoll steps
+// (k = 1, 1 + kStopPoll, ...): ctl points at the plan's control words in
+// mapped host memory, ctl[0] != 0 cancels, ctl[1] > 0 is each step kernel's
+// time budget in nanoseconds on the device's global timer, counted from that
+// kernel's start.  The kernel then records the status and the step and
+// leaves its loop as it does after a failed inversion.
+constexpr int kStopPoll = 128;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool stop_poll_step(int k) { return ((k - 1) % kStopPoll) == 0; }
+
+__device__ __forceinline__ int stop_requested(const volatile long long *ctl, unsigned long long t0)
+{
+    if (!ctl) return MGPU_OK;
+    if (ctl[0] != 0) return MGPU_ERR_CANCELLED;
+    const long long budget = ctl[1];
+    if (budget > 0 && (long long)(global_ns() - t0) > budget) return MGPU_ERR_DEADLINE;
+    return MGPU_OK;
 }
 
 }  // namespace mgpu

@@ -306,6 +306,21 @@ class Plan:
         if rc != 0:
             raise PropagatorError(f"run: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
 
+    def cancel(self, on: bool = True):
+        """Stop this plan's runs (in flight or later) with MGPU_ERR_CANCELLED
+        at the step kernels' next poll; cancel(False) clears the request.
+        Safe from another thread while run_host is waiting."""
+        rc = _lib.load().mgpu_plan_cancel(self._handle, 1 if on else 0)
+        if rc != 0:
+            raise PropagatorError(f"cancel: {_lib.status_string(rc)}", rc)
+
+    def set_time_limit(self, seconds: float):
+        """Stop jobs of a step kernel that runs longer than `seconds` with
+        MGPU_ERR_DEADLINE (0: no limit)."""
+        rc = _lib.load().mgpu_plan_set_time_limit(self._handle, float(seconds))
+        if rc != 0:
+            raise PropagatorError(f"time limit: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+
     def close(self):
         if self._handle:
             _lib.load().mgpu_plan_destroy(self._handle)
