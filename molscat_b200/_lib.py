@@ -58,11 +58,12 @@ _lib = None
 
 
 def load(path: str | None = None):
-    """Load the CUDA library (no compute call is made)."""
+    """Load the CUDA library (no compute call is made): `path`, else
+    $MOLSCAT_GPU_LIB, else the in-tree build."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB
+    p = path or os.environ.get("MOLSCAT_GPU_LIB") or LIB
     if not os.path.exists(p):
         raise ImportError(f"{p} is missing: build it with `python -m molscat_b200.build` "
                           "(there is no CPU fallback)")
