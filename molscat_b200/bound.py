@@ -64,19 +64,27 @@ def adiabatic_wkb_y(c: Coupling, r: float, p: np.ndarray, ered: float, outward: 
 
 @dataclass
 class BoundProblem:
-    """One (JTOT, block) system with its two propagation segments."""
+    """One (JTOT, block) system with its two propagation segments.
+
+    `inward(ered) -> (Y_in at RMATCH, NODES_in)`, when given, propagates the
+    long-range segment on the host instead of seg_in (BDPSET's IPROPL for a
+    propagator other than the log-derivative ones, e.g. AIRY); the GPU plan
+    then runs the outward segment alone."""
     coupling: Coupling
     seg_out: Segment  # RMIN -> RMATCH
-    seg_in: Segment   # RMAX -> RMATCH (DR < 0)
+    seg_in: Segment | None = None   # RMAX -> RMATCH (DR < 0)
     prop: str = "LDMD"
     y_out0: Callable[[float], np.ndarray] | None = None
     y_in0: Callable[[float], np.ndarray] | None = None
+    inward: Callable[[float], tuple] | None = None
 
     def __post_init__(self):
         c, so, si = self.coupling, self.seg_out, self.seg_in
+        if si is None and self.inward is None:
+            raise ValueError("BoundProblem needs seg_in or an inward propagator")
         if self.y_out0 is None:
             self.y_out0 = lambda e: adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
-        if self.y_in0 is None:
+        if self.y_in0 is None and si is not None:
             self.y_in0 = lambda e: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
 
 
@@ -85,23 +93,37 @@ def node_counts(bp: BoundProblem, ereds) -> tuple:
     eigenvalue) at every ERED, the propagations of all energies in one plan."""
     ereds = np.asarray(ereds, dtype=np.float64)
     m = ereds.size
-    job_sys = np.concatenate([np.zeros(m, dtype=np.int32), np.ones(m, dtype=np.int32)])
-    job_e = np.concatenate([ereds, ereds])
-    plan = Plan(bp.prop, [bp.coupling, bp.coupling], [bp.seg_out, bp.seg_in], job_sys, job_e)
+    host_in = bp.inward is not None
+    if host_in:
+        job_sys = np.zeros(m, dtype=np.int32)
+        job_e = ereds.copy()
+        plan = Plan(bp.prop, [bp.coupling], [bp.seg_out], job_sys, job_e)
+    else:
+        job_sys = np.concatenate([np.zeros(m, dtype=np.int32), np.ones(m, dtype=np.int32)])
+        job_e = np.concatenate([ereds, ereds])
+        plan = Plan(bp.prop, [bp.coupling, bp.coupling], [bp.seg_out, bp.seg_in], job_sys, job_e)
     try:
-        y0 = [bp.y_out0(float(e)) for e in ereds] + [bp.y_in0(float(e)) for e in ereds]
+        y0 = [bp.y_out0(float(e)) for e in ereds]
+        if not host_in:
+            y0 += [bp.y_in0(float(e)) for e in ereds]
         ybuf, nodes, status, kfail = plan.run_host(plan.pack(y0))
         if (status != 0).any():
             j = int(np.nonzero(status)[0][0])
             raise RuntimeError(f"propagation failed at ERED={job_e[j]} (status {int(status[j])}, step {int(kfail[j])})")
+        if host_in:
+            inner = [bp.inward(float(e)) for e in ereds]
+            y_in = [np.asarray(y) for y, _ in inner]
+            n_in = np.array([int(k) for _, k in inner], dtype=np.int64)
+        else:
+            y_in = [plan.unpack(ybuf, m + k) for k in range(m)]
+            n_in = nodes[m:].astype(np.int64)
         nmatch = np.zeros(m, dtype=np.int64)
         eigmin = np.zeros(m)
         for k in range(m):
-            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k))
+            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - y_in[k])
             nmatch[k] = int(np.sum(ev <= 0.0))
             eigmin[k] = ev[np.argmin(np.abs(ev))]
         n_out = nodes[:m].astype(np.int64)
-        n_in = nodes[m:].astype(np.int64)
         return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
     finally:
         plan.close()

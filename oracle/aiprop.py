@@ -43,6 +43,37 @@ def _w(c: O.Coupling, sysm, r: float, ered: float) -> np.ndarray:
     return O.hammat(c, r, sysm.pvec(r), ered)
 
 
+_Z_ASYM = 1.0e4  # above this the asymptotic series (4 terms) is exact to ~1e-22
+
+
+def _asym_coeffs(nterm: int = 4):
+    """u_k = Gamma(3k + 1/2) / (54^k k! Gamma(k + 1/2)), v_k = -(6k+1)/(6k-1) u_k
+    (Abramowitz and Stegun 10.4.58-10.4.67)."""
+    u = [1.0]
+    v = [1.0]
+    for k in range(1, nterm):
+        uk = math.exp(math.lgamma(3 * k + 0.5) - k * math.log(54.0) - math.lgamma(k + 1) - math.lgamma(k + 0.5))
+        u.append(uk)
+        v.append(-(6 * k + 1) / (6 * k - 1) * uk)
+    return u, v
+
+
+_U, _V = _asym_coeffs()
+
+
+def _airy_asym(z: np.ndarray):
+    """Scaled Ai, Ai', Bi, Bi' for large positive z from the asymptotic
+    series in 1/zeta (scipy's airye overflows internally near z ~ 1e6)."""
+    zeta = 2.0 / 3.0 * z * np.sqrt(z)
+    q = z ** 0.25
+    sp = math.sqrt(math.pi)
+    su_a = sum(((-1) ** k) * _U[k] / zeta ** k for k in range(len(_U)))
+    sv_a = sum(((-1) ** k) * _V[k] / zeta ** k for k in range(len(_V)))
+    su_b = sum(_U[k] / zeta ** k for k in range(len(_U)))
+    sv_b = sum(_V[k] / zeta ** k for k in range(len(_V)))
+    return su_a / (2.0 * sp * q), -q * sv_a / (2.0 * sp), su_b / (sp * q), q * sv_b / sp
+
+
 def _airy_all(z: np.ndarray):
     """(Ai, Ai', Bi, Bi') at z as mantissas with the growth exponent zeta+
     (zeta = 2/3 z^1.5 for z > 0, else 0): Ai = a e^-zeta+, Bi = b e^+zeta+."""
@@ -51,12 +82,14 @@ def _airy_all(z: np.ndarray):
     zp = np.where(z > 0.0, z, 0.0)
     zeta = 2.0 / 3.0 * zp * np.sqrt(zp)
     a, ap, b, bp = airy(np.where(z > 0.0, 0.0, z))
-    ea, eap, eb, ebp = airye(np.where(z > 0.0, z, 0.0))
-    pos = z > 0.0
-    a = np.where(pos, ea, a)
-    ap = np.where(pos, eap, ap)
-    b = np.where(pos, eb, b)
-    bp = np.where(pos, ebp, bp)
+    mid = (z > 0.0) & (z <= _Z_ASYM)
+    ea, eap, eb, ebp = airye(np.where(mid, z, 0.0))
+    big = z > _Z_ASYM
+    xa, xap, xb, xbp = _airy_asym(np.where(big, z, 2.0 * _Z_ASYM))
+    a = np.where(big, xa, np.where(mid, ea, a))
+    ap = np.where(big, xap, np.where(mid, eap, ap))
+    b = np.where(big, xb, np.where(mid, eb, b))
+    bp = np.where(big, xbp, np.where(mid, ebp, bp))
     return a, ap, b, bp, zeta
 
 
@@ -72,7 +105,7 @@ def _y124_mp(alpha, beta, width):
     the double inputs in mpmath, so their difference alpha*h keeps its
     digits however large z is."""
     import mpmath as mp
-    zeta = 2.0 / 3.0 * (abs(alpha) * (abs(beta) + width)) ** 1.5
+    zeta = 2.0 / 3.0 * (abs(alpha) * (abs(beta) + abs(width))) ** 1.5
     with mp.workdps(int(25 + 2 * math.log10(max(zeta, 10.0)))):
         al, be, h = mp.mpf(alpha), mp.mpf(beta), mp.mpf(width)
         z1 = al * (be - h / 2)
@@ -148,11 +181,15 @@ def _corr(eignow, eigold, hp, drnow, drmid, xlarge):
 
 def aiprop(c: O.Coupling, sysm, z: np.ndarray, rstart: float, rstop: float, drnow: float, ered: float,
            tolhi: float = 1.0e-4, powr: float = 3.0, maxstp: int = 500000):
-    """AIPROP from RSTART to RSTOP (outward), variable steps controlled by
-    TOLHI and POWR (aiprop.f:305-330).  z: log-derivative at RSTART in the
-    free basis.  Returns (Z at RSTOP, NODES, number of sectors)."""
-    if not (rstop > rstart):
-        raise ValueError("the restatement propagates outwards only")
+    """AIPROP from RSTART to RSTOP, outward or inward (DRNOW < 0), variable
+    steps controlled by TOLHI and POWR (aiprop.f:305-330).  z: log-derivative
+    at RSTART in the free basis.  Returns (Z at RSTOP, NODES, number of
+    sectors).  Inward, a sector adds N - KOUNT nodes (aiprop.f:196-200) and
+    the step factor carries (1 + DR/R)^3 for the rising potential
+    (aiprop.f:317-318)."""
+    if rstop == rstart or (rstop > rstart) != (drnow > 0.0):
+        raise ValueError("DRNOW must point from RSTART to RSTOP")
+    outward = rstop > rstart
     n = c.n
     z = np.array(z, dtype=np.float64)
     eigold = np.linalg.eigvalsh(-_w(c, sysm, rstart, ered))
@@ -180,7 +217,7 @@ def aiprop(c: O.Coupling, sysm, z: np.ndarray, rstart: float, rstop: float, drno
         inv, kount = O.syminv(a)
         if kount > n:
             raise RuntimeError("AIPROP: instability in SYMINV")
-        nodes += kount
+        nodes += kount if outward else n - kount
         inv = np.tril(inv) + np.tril(inv, -1).T
         z = -(y2[:, None] * inv * y2[None, :]) + np.diag(y4)
         if last:
@@ -188,6 +225,8 @@ def aiprop(c: O.Coupling, sysm, z: np.ndarray, rstart: float, rstop: float, drno
         if 0.0 < tolhi < 1.0:
             cmax = max(abs(cdiag), abs(coff))
             factor = 2.0 if cmax == 0.0 else (tolhi / cmax) ** (1.0 / powr)
+            if drnow < 0.0 and rnext + drnow > 0.0:
+                factor = factor * (1.0 + drnow / rnext) ** 3
             if factor > 2.0:
                 factor = 2.0
             drnow = drnow * factor
