@@ -29,21 +29,55 @@ from .propagators import Coupling, Plan, Segment
 
 @dataclass
 class FieldProblem:
-    """One (JTOT, block) at one energy, with its field-dependent coupling."""
+    """One (JTOT, block) at one energy, with its field-dependent coupling.
+
+    Where more than the coupling moves with the field, `segments_at(F) ->
+    (seg_out, seg_in)` gives the segments (their P tables hold any
+    field-dependent constant terms, e.g. a Zeeman prefactor) and
+    `ered_at(F)` the energy (an energy fixed relative to a field-dependent
+    threshold, the MONQN reference of fld.driver.f).  `inward(F, coupling,
+    ered) -> (Y_in at RMATCH, NODES_in)` propagates the long-range segment
+    on the host instead (e.g. AIRY); the plan then runs the outward segments
+    alone.  y_out0 / y_in0 default to the adiabatic WKB start."""
     coupling_at: Callable[[float], Coupling]
-    seg_out: Segment  # RMIN -> RMATCH
-    seg_in: Segment   # RMAX -> RMATCH (DR < 0)
-    ered: float
+    seg_out: Segment | None = None  # RMIN -> RMATCH
+    seg_in: Segment | None = None   # RMAX -> RMATCH (DR < 0)
+    ered: float = 0.0
     prop: str = "LDMD"
     y_out0: Callable[[Coupling], np.ndarray] | None = None
     y_in0: Callable[[Coupling], np.ndarray] | None = None
+    segments_at: Callable[[float], tuple] | None = None
+    ered_at: Callable[[float], float] | None = None
+    inward: Callable[[float, Coupling, float], tuple] | None = None
 
     def __post_init__(self):
-        so, si, e = self.seg_out, self.seg_in, self.ered
-        if self.y_out0 is None:
-            self.y_out0 = lambda c: adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
-        if self.y_in0 is None:
-            self.y_in0 = lambda c: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
+        if self.segments_at is None and self.seg_out is None:
+            raise ValueError("FieldProblem needs seg_out or segments_at")
+        if self.inward is None and self.segments_at is None and self.seg_in is None:
+            raise ValueError("FieldProblem needs seg_in, segments_at or an inward propagator")
+        if self.segments_at is None and self.ered_at is None:
+            so, si, e = self.seg_out, self.seg_in, self.ered
+            if self.y_out0 is None:
+                self.y_out0 = lambda c: adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
+            if self.y_in0 is None and si is not None:
+                self.y_in0 = lambda c: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
+
+    def at(self, f: float):
+        """(coupling, seg_out, seg_in, ERED) at field f."""
+        c = self.coupling_at(f)
+        so, si = self.segments_at(f) if self.segments_at is not None else (self.seg_out, self.seg_in)
+        e = self.ered_at(f) if self.ered_at is not None else self.ered
+        return c, so, si, e
+
+    def start_out(self, c, so, e):
+        if self.y_out0 is not None:
+            return self.y_out0(c)
+        return adiabatic_wkb_y(c, float(so.rtab[0]), so.ptab[0], e, True)
+
+    def start_in(self, c, si, e):
+        if self.y_in0 is not None:
+            return self.y_in0(c)
+        return adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
 
 
 def field_node_counts(fp: FieldProblem, fields) -> tuple:
@@ -52,24 +86,39 @@ def field_node_counts(fp: FieldProblem, fields) -> tuple:
     plan."""
     fields = np.asarray(fields, dtype=np.float64)
     m = fields.size
-    cs = [fp.coupling_at(float(f)) for f in fields]
-    job_sys = np.arange(2 * m, dtype=np.int32)
-    plan = Plan(fp.prop, cs + cs, [fp.seg_out] * m + [fp.seg_in] * m, job_sys, np.full(2 * m, fp.ered))
+    sys_at = [fp.at(float(f)) for f in fields]
+    cs = [a[0] for a in sys_at]
+    outs = [a[1] for a in sys_at]
+    ins = [a[2] for a in sys_at]
+    es = np.array([a[3] for a in sys_at], dtype=np.float64)
+    host_in = fp.inward is not None
+    if host_in:
+        plan = Plan(fp.prop, cs, outs, np.arange(m, dtype=np.int32), es)
+    else:
+        plan = Plan(fp.prop, cs + cs, outs + ins, np.arange(2 * m, dtype=np.int32), np.concatenate([es, es]))
     try:
-        y0 = [fp.y_out0(c) for c in cs] + [fp.y_in0(c) for c in cs]
+        y0 = [fp.start_out(c, so, e) for c, so, e in zip(cs, outs, es)]
+        if not host_in:
+            y0 += [fp.start_in(c, si, e) for c, si, e in zip(cs, ins, es)]
         ybuf, nodes, status, kfail = plan.run_host(plan.pack(y0))
         if (status != 0).any():
             j = int(np.nonzero(status)[0][0])
             raise RuntimeError(f"propagation failed at F={fields[j % m]} (status {int(status[j])}, "
                                f"step {int(kfail[j])})")
+        if host_in:
+            inner = [fp.inward(float(f), c, float(e)) for f, c, e in zip(fields, cs, es)]
+            y_in = [np.asarray(y) for y, _ in inner]
+            n_in = np.array([int(k) for _, k in inner], dtype=np.int64)
+        else:
+            y_in = [plan.unpack(ybuf, m + k) for k in range(m)]
+            n_in = nodes[m:].astype(np.int64)
         nmatch = np.zeros(m, dtype=np.int64)
         eigmin = np.zeros(m)
         for k in range(m):
-            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k))
+            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - y_in[k])
             nmatch[k] = int(np.sum(ev <= 0.0))
             eigmin[k] = ev[np.argmin(np.abs(ev))]
         n_out = nodes[:m].astype(np.int64)
-        n_in = nodes[m:].astype(np.int64)
         return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
     finally:
         plan.close()

@@ -179,14 +179,60 @@ def _corr(eignow, eigold, hp, drnow, drmid, xlarge):
     return cdiag, coff
 
 
+def drcalc(rstart: float, rstop: float, kstep: int, nstep: int, pow_: float) -> float:
+    """Size of step KSTEP (0-based) when the step boundaries are equally
+    spaced in R^(1-POW) (drcalc.f:22-38)."""
+    powint = 1.0 - pow_
+    powinv = 1.0 / powint
+    if powint != 0.0:
+        zstart = rstart ** powint
+        zstop = rstop ** powint
+        dz = (zstop - zstart) / float(nstep)
+        rnow = (zstart + float(kstep + 1) * dz) ** powinv
+        rlast = (zstart + float(kstep) * dz) ** powinv
+        return rnow - rlast
+    dz = rstart * ((rstop / rstart) ** (1.0 / float(nstep)) - 1.0)
+    return dz * (1.0 + dz / rstart) ** kstep
+
+
+def drset(rstart: float, rstop: float, drfit: float, tolhi: float, pow_: float):
+    """(NSTEP, first DR) of a segment whose step is set from DRS/DRL
+    (drset.f:54-84): with TOLHI = 0 a whole number of steps scaling as
+    R^POW, the first one DR; with 0 < TOLHI < 1 just DRFIT (NSTEP 0)."""
+    rsmall = min(rstart, rstop)
+    rlarge = max(rstart, rstop)
+    powint = 1.0 - pow_
+    prange = rlarge - rsmall
+    nstep = 0
+    dr = drfit
+    if tolhi == 0.0:
+        rratio = drfit / rsmall
+        if pow_ == 0.0:
+            nstep = max(O.nint(prange / drfit), 1)
+            dr = prange / float(nstep)
+        elif pow_ == 1.0:
+            nstep = O.nint(math.log(rlarge / rsmall) / math.log(rratio + 1.0))
+            dr = drcalc(rstart, rstop, 0, nstep, pow_)
+        else:
+            zrm1 = (rlarge / rsmall) ** powint - 1.0
+            nstep = O.nint(zrm1 / ((rratio + 1.0) ** powint - 1.0))
+            dr = drcalc(rstart, rstop, 0, nstep, pow_)
+    if rstop < rstart:
+        dr = -abs(dr)
+    return nstep, dr
+
+
 def aiprop(c: O.Coupling, sysm, z: np.ndarray, rstart: float, rstop: float, drnow: float, ered: float,
-           tolhi: float = 1.0e-4, powr: float = 3.0, maxstp: int = 500000):
+           tolhi: float = 1.0e-4, powr: float = 3.0, maxstp: int = 500000, nstep: int = 0):
     """AIPROP from RSTART to RSTOP, outward or inward (DRNOW < 0), variable
-    steps controlled by TOLHI and POWR (aiprop.f:305-330).  z: log-derivative
-    at RSTART in the free basis.  Returns (Z at RSTOP, NODES, number of
-    sectors).  Inward, a sector adds N - KOUNT nodes (aiprop.f:196-200) and
-    the step factor carries (1 + DR/R)^3 for the rising potential
-    (aiprop.f:317-318)."""
+    steps controlled by TOLHI and POWR (aiprop.f:305-330), or with TOLHI = 0
+    NSTEP steps scaling as R^POWR (DRCALC, aiprop.f:320-328).  z:
+    log-derivative at RSTART in the free basis.  Returns (Z at RSTOP, NODES,
+    number of sectors).  Inward, a sector adds N - KOUNT nodes
+    (aiprop.f:196-200) and the step factor carries (1 + DR/R)^3 for the
+    rising potential (aiprop.f:317-318)."""
+    if tolhi == 0.0 and nstep < 1:
+        raise ValueError("TOLHI = 0 needs NSTEP (drset)")
     if rstop == rstart or (rstop > rstart) != (drnow > 0.0):
         raise ValueError("DRNOW must point from RSTART to RSTOP")
     outward = rstop > rstart
@@ -233,8 +279,13 @@ def aiprop(c: O.Coupling, sysm, z: np.ndarray, rstart: float, rstop: float, drno
             rlast = rnext
             rnext = rnext + drnow
             last = (rstop - rstart) * (rstop - rnext) < 0.0
+        elif tolhi == 0.0:
+            drnow = drcalc(rstart, rstop, kstep, nstep, powr)
+            rlast = rnext
+            rnext = rnext + drnow
+            last = nstep - kstep <= 1
         else:
-            raise ValueError("the restatement covers 0 < TOLHI < 1")
+            raise ValueError("the restatement covers 0 <= TOLHI < 1")
         if last:
             rnext = rstop
             drnow = rnext - rlast

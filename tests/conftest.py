@@ -1,7 +1,11 @@
 import os
 import sys
 
-import pytest
+# the oracle's small dense solves run fastest single-threaded; many BLAS
+# threads per process only contend with the GPU tests' host threads
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+import pytest  # noqa: E402
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:

@@ -1,6 +1,6 @@
-"""Extract the bound-Mg_NH example (ITYPE=9 atom + 3Sigma diatom in a
-magnetic field, N = 100 channels, MDPROP outward + AIRY inward) into a
-committed fixture.
+"""Extract the bound-Mg_NH and field-Mg_NH examples (ITYPE=9 atom + 3Sigma
+diatom in a magnetic field, N = 100 channels, MDPROP outward + AIRY inward)
+into committed fixtures.
 
 Run with the reference project's checkout named by $MOLSCAT_REF (required):
 
@@ -15,7 +15,14 @@ writes tests/golden/bound_mg_nh.json with
   eigenvalue's index;
 * the potential's angular cuts (angle, R, E) read from data/pot-Mg_NH.data,
   the input of the RKHS interpolation (first two columns: R and EINT1, as
-  vstar-Mg_NH.f reads them).
+  vstar-Mg_NH.f reads them);
+
+and tests/golden/field_mg_nh.json with the parameters of
+examples/input/field-Mg_NH.input (energies relative to the field-dependent
+threshold, FLDMIN/FLDMAX, DTOL, TOLHIL = 0) and, per energy of
+examples/output/field-Mg_NH.output, the node counts at FLDMIN and FLDMAX and
+the converged field of each state (the same system and potential as the
+bound fixture).
 """
 import json
 import os
@@ -26,6 +33,7 @@ REF = os.environ.get("MOLSCAT_REF")
 if not REF:
     sys.exit("set MOLSCAT_REF to the reference project's checkout")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bound_mg_nh.json")
+OUT_FIELD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "field_mg_nh.json")
 
 
 def _num(text, name):
@@ -95,6 +103,26 @@ def read_cuts():
     return cuts
 
 
+def read_field():
+    with open(os.path.join(REF, "examples", "input", "field-Mg_NH.input")) as f:
+        t = f.read()
+    inp = {"rmin": _num(t, "RMIN"), "rmatch": _num(t, "RMATCH"), "rmax": _num(t, "RMAX"), "drs": _num(t, "DRS"),
+           "drl": _num(t, "DRL"), "tolhil": _num(t, "TOLHIL"), "fldmin": _num(t, "FLDMIN"),
+           "fldmax": _num(t, "FLDMAX"), "dtol_g": _num(t, "DTOL"),
+           "energies_mhz": _list(t, "ENERGY")[: int(_num(t, "NNRG"))]}
+    with open(os.path.join(REF, "examples", "output", "field-Mg_NH.output")) as f:
+        o = f.read()
+    inp["powrl"] = 4.0 / 3.0 if re.search(r"STEP SIZE SCALES AS R\*\*1\.33", o) else None
+    per = []
+    for body in re.split(r"ENERGY\s+\d+ =", o)[1:]:
+        cnt = [int(x) for x in re.findall(r"IMPLIES\s+(\d+) STATES BELOW SPECIFIED ENERGY", body)]
+        states = [{"state": int(m.group(1)), "field_g": float(m.group(2))} for m in
+                  re.finditer(r"CONVERGED ON STATE NUMBER\s+(\d+) AT\s+MAGNETIC Z FIELD =\s+(\S+)", body)]
+        per.append({"energy_mhz": float(body.split()[0]), "count_fldmin": cnt[0], "count_fldmax": cnt[1],
+                    "states": states})
+    return inp, per
+
+
 def main():
     inp = read_input()
     block, nchan, sets = read_output()
@@ -104,6 +132,12 @@ def main():
     with open(OUT, "w") as f:
         json.dump(g, f, indent=1)
     print(OUT, len(sets), "field sets,", len(g["cuts"]), "cuts")
+    finp, per = read_field()
+    fg = {"source": "examples/input/field-Mg_NH.input, examples/output/field-Mg_NH.output",
+          "system": finp, "energies": per}
+    with open(OUT_FIELD, "w") as f:
+        json.dump(fg, f, indent=1)
+    print(OUT_FIELD, len(per), "energies")
 
 
 if __name__ == "__main__":
