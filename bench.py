@@ -74,6 +74,10 @@ def parse():
     ap.add_argument("--leg-large-n", default="512,1024")
     ap.add_argument("--leg-large-energies", type=int, default=64)
     ap.add_argument("--leg-large-nstep", type=int, default=300)
+    ap.add_argument("--no-fields", action="store_true", help="skip the BOUND/FIELD field-sweep leg")
+    ap.add_argument("--leg-fields", type=int, default=2048, help="fields of the alkali-pair sweep (0-1000 G)")
+    ap.add_argument("--leg-field-nout", type=int, default=1800)
+    ap.add_argument("--leg-field-nin", type=int, default=2400)
     return ap.parse_args()
 
 
@@ -498,6 +502,103 @@ def large_leg(ns, energies: int, nstep: int, reps: int, peak: float | None = Non
             "clocks": clk}
 
 
+def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = None) -> dict:
+    """The BOUND/FIELD workload: the synthetic alkali pair (i = 3/2 on both
+    atoms, N = 106) at E = 0 relative to its lowest threshold, counted at
+    `nfield` fields in 0-1000 G.  Every field is a system; all share VL, P and
+    the MDPROP U(C) preparation (the Zeeman term is a per-field EINT), so one
+    plan runs 2 x nfield propagations (outward and inward) after two
+    preparations.  The state count at a field is NODES_out + NODES_in + the
+    non-positive eigenvalues of Y_out - Y_in; where it changes between
+    neighbouring fields a bound state crosses threshold (a resonance field)."""
+    import torch
+    from molscat_b200.alkali import config4_sweep
+    from molscat_b200.propagators import Plan
+    t0 = time.perf_counter()
+    sw = config4_sweep(nout=nout, nin=nin)
+    fields = np.linspace(0.0, 1000.0, nfield)
+    cs = [sw.coupling_at(float(f)) for f in fields]
+    es = np.array([sw.ered_at(float(f)) for f in fields])
+    m = nfield
+    plan = Plan("LDMD", cs + cs, [sw.seg_out] * m + [sw.seg_in] * m, np.arange(2 * m), np.concatenate([es, es]))
+
+    def starts():
+        # adiabatic WKB starts (yinit.f with ADIAMN), all fields in one batched eigh per end
+        from molscat_b200.bound import w_matrix
+        ys = []
+        for seg, sgn in ((sw.seg_out, 1.0), (sw.seg_in, -1.0)):
+            w = np.stack([w_matrix(c, float(seg.rtab[0]), seg.ptab[0], e) for c, e in zip(cs, es)])
+            lam, vec = np.linalg.eigh(w)
+            yl = np.where(lam > 0.0, sgn * np.sqrt(np.abs(lam)), 0.0)
+            ys += list(np.einsum("fij,fj,fkj->fik", vec, yl, vec))
+        return ys
+
+    def counts(ybuf, nodes):
+        yo = np.stack([plan.unpack(ybuf, k) for k in range(m)])
+        yi = np.stack([plan.unpack(ybuf, m + k) for k in range(m)])
+        ev = np.linalg.eigvalsh(yo - yi)
+        return nodes[:m].astype(np.int64) + nodes[m:] + np.sum(ev <= 0.0, axis=1)
+
+    y0 = plan.pack(starts())
+    t_setup = time.perf_counter() - t0
+    dev = torch.device("cuda:0")
+    y0d = torch.from_numpy(y0).to(dev)
+    y = torch.empty_like(y0d)
+    nd = torch.zeros(2 * m, dtype=torch.int32, device=dev)
+    st, kf = torch.zeros_like(nd), torch.zeros_like(nd)
+    sp = torch.cuda.current_stream().cuda_stream
+    y.copy_(y0d)
+    plan.run_device(y.data_ptr(), nd.data_ptr(), st.data_ptr(), kf.data_ptr(), sp, phases=3)
+    torch.cuda.synchronize()
+    if (st.cpu().numpy() != 0).any():
+        raise RuntimeError("field-sweep propagation failed")
+    clocks = ClockSampler(0)
+    clocks.start()
+    prep, prop = [], []
+    for _ in range(max(1, reps)):
+        y.copy_(y0d)
+        a0, a1, a2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        a0.record()
+        plan.run_device(y.data_ptr(), nd.data_ptr(), st.data_ptr(), kf.data_ptr(), sp, phases=1)
+        a1.record()
+        plan.run_device(y.data_ptr(), nd.data_ptr(), st.data_ptr(), kf.data_ptr(), sp, phases=2)
+        a2.record()
+        a2.synchronize()
+        prep.append(a0.elapsed_time(a1))
+        prop.append(a1.elapsed_time(a2))
+    clk = clocks.stop()
+    # end to end through the C ABI with host buffers, then the matching on the host
+    ta = time.perf_counter()
+    ybuf, nodes, status, _ = plan.run_host(y0)
+    tb = time.perf_counter()
+    cnt = counts(ybuf, nodes)
+    tc = time.perf_counter()
+    if (status != 0).any():
+        raise RuntimeError("field-sweep propagation failed")
+    steps = [(f, int(cnt[k]), int(cnt[k + 1])) for k, f in enumerate(fields[:-1]) if cnt[k] != cnt[k + 1]]
+    t_prep, t_prop = statistics.mean(prep), statistics.mean(prop)
+    work = float(m) * sw.n ** 3 * (nout + nin)
+    tfl = plan.flops_prop / (t_prop * 1e-3) / 1e12
+    out = {"fields": m, "n": sw.n, "propagations": 2 * m, "shared_systems": plan.shared_systems,
+           "prep_ms": t_prep, "prop_ms": t_prop, "fields_per_s": m / ((t_prep + t_prop) * 1e-3),
+           "channel3_steps_per_s": work / ((t_prep + t_prop) * 1e-3), "prop_tflops": tfl,
+           "prop_frac": (tfl * 1e12 / peak) if peak else None,
+           "e2e": {"s": tc - ta, "run_host_s": tb - ta, "matching_s": tc - tb, "fields_per_s": m / (tc - ta),
+                   "h2d_bytes": int(plan.y_elems * 8), "d2h_bytes": int(plan.y_elems * 8 + 3 * 4 * 2 * m)},
+           "count_range": [int(cnt.min()), int(cnt.max())], "crossings": len(steps),
+           "first_crossings_g": [round(float(f), 3) for f, _, _ in steps[:8]],
+           "setup_s": t_setup, "clocks": clk,
+           "config": {"workload": "alkali pair in the uncoupled basis (base9-alk_alk_ucpld form), s = 1/2, i = 3/2 "
+                                  "on both atoms, hyperfine 1.0 / 0.8 GHz, L <= 4, MTOT = 2 (M_F), even L: N = %d; "
+                                  "Morse singlet/triplet (De 3900/240 cm-1, Re 4.2/6.0 A) with damped -C6/R^6, "
+                                  "C6 = 4700 Eh a0^6; E = 0 at the lowest threshold; %d fields 0-1000 G; MDPROP "
+                                  "3 -> 12 A (%d steps) and 60 -> 12 A (%d steps)" % (sw.n, m, nout, nin)}}
+    plan.close()
+    del y0d, y
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_large(args):
     """--workload large: the large-N leg alone, with its own flags."""
     import torch
@@ -729,6 +830,8 @@ def main():
             ns = [int(x) for x in args.leg_large_n.split(",")]
             line["large_n"] = large_leg(ns, args.leg_large_energies, args.leg_large_nstep, 2, peak=peak)
             line["large_n"]["peak_source"] = line["roofline"]["peak_source"]
+        if not args.no_fields:
+            line["field_sweep"] = field_leg(args.leg_fields, args.leg_field_nout, args.leg_field_nin, 2, peak=peak)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -20,9 +20,11 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "molscat_gpu.h"
@@ -972,6 +974,8 @@ struct mgpu_plan {
     int iprop = 0;
     int nsys = 0, njobs = 0;
     std::vector<int> sys_n, sys_bucket, sys_nstep, sys_nham;
+    std::vector<int> sys_owner;    // the system whose tables (and U(C) preparation) this one uses; itself if none
+    int nshared = 0;               // systems using another's tables
     std::vector<size_t> yoff;      // per job, caller order
     size_t yelems = 0;
     double flops = 0.0;       // 3N^3 + 2 NHAM N(N+1) per job step (the reference's count)
@@ -1171,6 +1175,21 @@ static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, i
     d.q = dq;
     d.ctl = nullptr;
     return MGPU_OK;
+}
+
+// Two systems share device tables when they differ at most in EINT and CENT:
+// the same VL, IV, P and R arrays (by address) and the same sizes and flags.
+// EINT and CENT enter W only on its diagonal, and MDPROP's U(C) uses only the
+// off-diagonal coupling (mdprop.f:104-130), so such systems also share the
+// 2HQ(C) tables and their preparation.  A field sweep in a basis where the
+// field term is diagonal (the uncoupled alkali-pair basis, whose Zeeman term
+// becomes a per-field EINT) is the case this serves: one preparation for
+// every field.
+static bool shares_tables(const mgpu_coupling &a, const mgpu_grid &ga, const mgpu_coupling &b, const mgpu_grid &gb)
+{
+    return a.n == b.n && a.nham == b.nham && a.nvlblk == b.nvlblk && a.ivlfl == b.ivlfl && a.nconst == b.nconst &&
+           a.nrsq == b.nrsq && a.conlen == b.conlen && a.vl == b.vl && (a.ivlfl <= 0 || a.iv == b.iv) &&
+           ga.nstep == gb.nstep && ga.dr == gb.dr && ga.rtab == gb.rtab && ga.ptab == gb.ptab;
 }
 
 constexpr int kPrepChunk = 128;  // U(C) steps inverted per preparation batch
@@ -1475,6 +1494,8 @@ size_t mgpu_plan_y_offset(const mgpu_plan *p, int job)
 
 double mgpu_plan_flops(const mgpu_plan *p) { return p ? p->flops : 0.0; }
 
+int mgpu_plan_shared_systems(const mgpu_plan *p) { return p ? p->nshared : 0; }
+
 double mgpu_plan_flops_phase(const mgpu_plan *p, int phases)
 {
     if (!p) return 0.0;
@@ -1538,13 +1559,47 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
     };
     std::vector<SysDev> hs(nsys);
+    // owners by table identity (pointer and scalar key), large-N buckets excluded
+    std::map<std::tuple<const double *, const int *, const double *, const double *, int, int, int>, std::vector<int>>
+        owners_by_key;
     for (int s = 0; s < nsys; ++s) {
         const int b = bucket_for(systems[s].n, iprop);
         p->sys_n.push_back(systems[s].n);
         p->sys_bucket.push_back(b);
         p->sys_nstep.push_back(grids[s].nstep);
         p->sys_nham.push_back(systems[s].nham);
-        const int rc = build_sysdev(systems[s], grids[s], iprop, b, hs[s], sync_alloc, sync_upload);
+        int owner = s;
+        if (kBuckets[b].kind != KIND_BIG) {
+            auto &cand = owners_by_key[std::make_tuple(systems[s].vl, systems[s].iv, grids[s].ptab, grids[s].rtab,
+                                                       systems[s].n, grids[s].nstep, b)];
+            for (int r : cand)
+                if (shares_tables(systems[r], grids[r], systems[s], grids[s])) {
+                    owner = r;
+                    break;
+                }
+            if (owner == s) cand.push_back(s);
+        }
+        p->sys_owner.push_back(owner);
+        int rc;
+        if (owner == s) {
+            rc = build_sysdev(systems[s], grids[s], iprop, b, hs[s], sync_alloc, sync_upload);
+        } else {
+            // the owner's tables; this system's own EINT and CENT
+            hs[s] = hs[owner];
+            const int npad = bucket_npad(b);
+            std::vector<double> eint(npad, 0.0), cent(npad, 0.0);
+            std::copy(systems[s].eint, systems[s].eint + systems[s].n, eint.begin());
+            std::copy(systems[s].cent, systems[s].cent + systems[s].n, cent.begin());
+            double *de = nullptr, *dc = nullptr;
+            cudaError_t e2;
+            rc = MGPU_OK;
+            if ((e2 = put_n(sync_alloc, sync_upload, &de, eint.data(), eint.size())) ||
+                (e2 = put_n(sync_alloc, sync_upload, &dc, cent.data(), cent.size())))
+                rc = set_err(MGPU_ERR_NOMEM, "uploading a system", e2);
+            hs[s].eint = de;
+            hs[s].cent = dc;
+            ++p->nshared;
+        }
         if (rc) {
             delete p;
             return rc;
@@ -1552,6 +1607,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     }
     if (iprop == MGPU_PROP_LDMD)
         for (int s = 0; s < nsys; ++s) {
+            if (p->sys_owner[s] != s) continue;
             const double n = systems[s].n, nh = systems[s].nham;
             p->flops_prep += (n * n * n + nh * n * (n + 1.0)) * grids[s].nstep;
         }
@@ -1559,7 +1615,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         delete p;
         return set_err(MGPU_ERR_NOMEM, "allocating prep counters", e);
     }
-    for (int s = 0; s < nsys; ++s) hs[s].prep = p->d_prep + 3 * s;
+    for (int s = 0; s < nsys; ++s) hs[s].prep = p->d_prep + 3 * p->sys_owner[s];
     {
         void *h = nullptr, *dptr = nullptr;
         if ((e = cudaHostAlloc(&h, 2 * sizeof(long long), cudaHostAllocMapped)) ||
@@ -1617,7 +1673,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
             }
         int sb = (int)syslist.size(), sc = 0, mx = 0, nhmax = 0;
         for (int s = 0; s < nsys; ++s)
-            if (p->sys_bucket[s] == b) {
+            if (p->sys_bucket[s] == b && p->sys_owner[s] == s) {  // prepared once per owner
                 syslist.push_back(s);
                 ++sc;
                 mx = std::max(mx, p->sys_nstep[s]);

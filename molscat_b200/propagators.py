@@ -233,6 +233,7 @@ class Plan:
         self.y_elems = int(L.mgpu_plan_y_elems(h))
         self.offsets = np.array([L.mgpu_plan_y_offset(h, j) for j in range(len(self.job_sys))], dtype=np.int64)
         self.flops = float(L.mgpu_plan_flops(h))
+        self.shared_systems = int(L.mgpu_plan_shared_systems(h))
         self.launches = int(L.mgpu_plan_launches(h))
         self.flops_prep = float(L.mgpu_plan_flops_phase(h, 1))
         self.flops_prop = float(L.mgpu_plan_flops_phase(h, 2))
