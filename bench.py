@@ -533,11 +533,19 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
             ys += list(np.einsum("fij,fj,fkj->fik", vec, yl, vec))
         return ys
 
-    def counts(ybuf, nodes):
+    def counts_host(ybuf, nodes):
         yo = np.stack([plan.unpack(ybuf, k) for k in range(m)])
         yi = np.stack([plan.unpack(ybuf, m + k) for k in range(m)])
         ev = np.linalg.eigvalsh(yo - yi)
         return nodes[:m].astype(np.int64) + nodes[m:] + np.sum(ev <= 0.0, axis=1)
+
+    pairs = np.stack([np.arange(m), np.arange(m, 2 * m)], axis=1)
+
+    def counts_device(ybuf, nodes):
+        mc = plan.match_counts(pairs).astype(np.int64)
+        for k in np.nonzero(mc < 0)[0]:  # a zero pivot: count from the eigenvalues
+            mc[k] = int(np.sum(np.linalg.eigvalsh(plan.unpack(ybuf, k) - plan.unpack(ybuf, m + k)) <= 0.0))
+        return nodes[:m].astype(np.int64) + nodes[m:] + mc
 
     y0 = plan.pack(starts())
     t_setup = time.perf_counter() - t0
@@ -571,10 +579,13 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
     ta = time.perf_counter()
     ybuf, nodes, status, _ = plan.run_host(y0)
     tb = time.perf_counter()
-    cnt = counts(ybuf, nodes)
+    cnt = counts_device(ybuf, nodes)
     tc = time.perf_counter()
     if (status != 0).any():
         raise RuntimeError("field-sweep propagation failed")
+    th = time.perf_counter()
+    cnt_host = counts_host(ybuf, nodes)
+    t_host_match = time.perf_counter() - th
     steps = [(f, int(cnt[k]), int(cnt[k + 1])) for k, f in enumerate(fields[:-1]) if cnt[k] != cnt[k + 1]]
     t_prep, t_prop = statistics.mean(prep), statistics.mean(prop)
     work = float(m) * sw.n ** 3 * (nout + nin)
@@ -584,7 +595,10 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
            "channel3_steps_per_s": work / ((t_prep + t_prop) * 1e-3), "prop_tflops": tfl,
            "prop_frac": (tfl * 1e12 / peak) if peak else None,
            "e2e": {"s": tc - ta, "run_host_s": tb - ta, "matching_s": tc - tb, "fields_per_s": m / (tc - ta),
-                   "h2d_bytes": int(plan.y_elems * 8), "d2h_bytes": int(plan.y_elems * 8 + 3 * 4 * 2 * m)},
+                   "h2d_bytes": int(plan.y_elems * 8), "d2h_bytes": int(plan.y_elems * 8 + 3 * 4 * 2 * m),
+                   "api": "mgpu_plan_run_host, then mgpu_plan_match_counts (LDL^T inertia of Y_out - Y_in on "
+                          "the device)"},
+           "matching_host_eigvalsh_s": t_host_match, "device_counts_equal_host": bool(np.array_equal(cnt, cnt_host)),
            "count_range": [int(cnt.min()), int(cnt.max())], "crossings": len(steps),
            "first_crossings_g": [round(float(f), 3) for f, _, _ in steps[:8]],
            "setup_s": t_setup, "clocks": clk,

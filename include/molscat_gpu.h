@@ -130,6 +130,19 @@ double mgpu_plan_flops(const mgpu_plan *plan);            /* counted FP64 work (
  * tables and preparation (U uses only the off-diagonal coupling). */
 int mgpu_plan_shared_systems(const mgpu_plan *plan);
 
+/* BOUND/FIELD matching counts (bdctrl.f:221-257): for each pair k of jobs
+ * (pairs[2k], pairs[2k+1], the same N <= 240) the number of negative
+ * eigenvalues of Y_a - Y_b, from the inertia of an unpivoted LDL^T of the
+ * difference on the device (Sylvester's law); -1 where a pivot is exactly
+ * zero or not finite, for the caller to count from the eigenvalues.  The
+ * _device form reads Y from y_dev laid out as the plan's Y buffer, with pairs
+ * and counts in device memory, on `stream`; mgpu_plan_match_counts reads the
+ * Y of the plan's last mgpu_plan_run_host from device memory (host pairs and
+ * counts, synchronous). */
+int mgpu_plan_match_counts_device(mgpu_plan *plan, const double *y_dev, int npairs, const int *pairs_dev,
+                                  int *counts_dev, void *stream);
+int mgpu_plan_match_counts(mgpu_plan *plan, int npairs, const int *pairs, int *counts);
+
 /* Host buffers: copies Y in, runs every job, copies Y, NODES and status out. */
 int mgpu_plan_run_host(mgpu_plan *plan, double *y, int *nodes, int *status, int *kfail);
 

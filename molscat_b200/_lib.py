@@ -44,7 +44,8 @@ class Grid_C(ctypes.Structure):
 EXPORTS = (
     "mgpu_mdprop", "mgpu_ldprop",
     "mgpu_plan_create", "mgpu_plan_destroy", "mgpu_plan_y_elems", "mgpu_plan_y_offset",
-    "mgpu_plan_flops", "mgpu_plan_shared_systems", "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
+    "mgpu_plan_flops", "mgpu_plan_shared_systems", "mgpu_plan_match_counts", "mgpu_plan_match_counts_device",
+    "mgpu_plan_run_host", "mgpu_plan_run_device", "mgpu_plan_launches",
     "mgpu_plan_run_device_phases", "mgpu_plan_flops_phase", "mgpu_probe_fp64_fma",
     "mgpu_status_string", "mgpu_last_error", "mgpu_max_n", "mgpu_mdprop_noalloc", "mgpu_set_kernel_family",
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
@@ -83,6 +84,8 @@ def load(path: str | None = None):
     L.mgpu_plan_flops.argtypes = [vp]
     L.mgpu_plan_flops.restype = ctypes.c_double
     L.mgpu_plan_shared_systems.argtypes = [vp]
+    L.mgpu_plan_match_counts.argtypes = [vp, ctypes.c_int, _ip, _ip]
+    L.mgpu_plan_match_counts_device.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
     L.mgpu_plan_run_host.argtypes = [vp, _dp, _ip, _ip, _ip]
     L.mgpu_plan_run_device.argtypes = [vp, vp, vp, vp, vp, vp]
     L.mgpu_plan_launches.argtypes = [vp]

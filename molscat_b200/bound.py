@@ -22,7 +22,8 @@ from typing import Callable
 
 import numpy as np
 
-from .propagators import Coupling, Plan, Segment
+from ._lib import MGPU_ERR_UNSUPPORTED
+from .propagators import Coupling, Plan, PropagatorError, Segment
 
 
 def w_matrix(c: Coupling, r: float, p: np.ndarray, ered: float) -> np.ndarray:
@@ -88,9 +89,11 @@ class BoundProblem:
             self.y_in0 = lambda e: adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
 
 
-def node_counts(bp: BoundProblem, ereds) -> tuple:
+def node_counts(bp: BoundProblem, ereds, eig: bool = True) -> tuple:
     """(counts, NODES_out, NODES_in, matching counts, smallest matching
-    eigenvalue) at every ERED, the propagations of all energies in one plan."""
+    eigenvalue) at every ERED, the propagations of all energies in one plan.
+    eig=False counts the matching matrices' negative eigenvalues on the
+    device (LDL^T inertia) and returns NaN for the smallest eigenvalues."""
     ereds = np.asarray(ereds, dtype=np.float64)
     m = ereds.size
     host_in = bp.inward is not None
@@ -117,16 +120,34 @@ def node_counts(bp: BoundProblem, ereds) -> tuple:
         else:
             y_in = [plan.unpack(ybuf, m + k) for k in range(m)]
             n_in = nodes[m:].astype(np.int64)
-        nmatch = np.zeros(m, dtype=np.int64)
-        eigmin = np.zeros(m)
-        for k in range(m):
-            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - y_in[k])
-            nmatch[k] = int(np.sum(ev <= 0.0))
-            eigmin[k] = ev[np.argmin(np.abs(ev))]
+        nmatch, eigmin = matching_counts(plan, ybuf, y_in, m, eig, host_in)
         n_out = nodes[:m].astype(np.int64)
         return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
     finally:
         plan.close()
+
+
+def matching_counts(plan, ybuf, y_in, m: int, eig: bool, host_in: bool):
+    """Non-positive eigenvalue counts of Y_out - Y_in (job k against job
+    m + k, or the host's Y_in) and the smallest-magnitude eigenvalues (NaN
+    when eig is False: the counts then come from the device)."""
+    nmatch = np.zeros(m, dtype=np.int64)
+    eigmin = np.full(m, np.nan)
+    dev = None
+    if not eig and not host_in and m > 0:
+        try:
+            dev = plan.match_counts(np.stack([np.arange(m), np.arange(m, 2 * m)], axis=1))
+        except PropagatorError as err:  # N above the kernel's limit: count on the host
+            if err.status != MGPU_ERR_UNSUPPORTED:
+                raise
+    for k in range(m):
+        if dev is not None and dev[k] >= 0:
+            nmatch[k] = int(dev[k])
+            continue
+        ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - y_in[k])
+        nmatch[k] = int(np.sum(ev <= 0.0))
+        eigmin[k] = ev[np.argmin(np.abs(ev))]
+    return nmatch, eigmin
 
 
 def bisect_steps(count: Callable, lo: float, hi: float, c_lo: int, c_hi: int, tol: float,
@@ -284,7 +305,7 @@ def find_states(bp: BoundProblem, emin: float, emax: float, tol: float, max_roun
     the state where the count steps from k to k+1 (the reference prints it as
     state number k+1), at the bracket midpoint.  `counter(bp, ereds) ->
     counts` defaults to the GPU node count."""
-    count = counter or (lambda b, e: node_counts(b, e)[0])
+    count = counter or (lambda b, e: node_counts(b, e, eig=False)[0])
     c0, c1 = (int(x) for x in count(bp, [emin, emax]))
     return bisect_steps(lambda xs: count(bp, xs), emin, emax, c0, c1, tol, max_rounds)
 

@@ -579,6 +579,7 @@ ldj_prop_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ j
 #include "kernels_cta.cuh"
 #include "kernels_big.cuh"
 #include "kernels_smatrix.cuh"
+#include "kernels_match.cuh"
 namespace mgpu {
 
 __global__ void prep_reset_kernel(int *prep, int nsys)
@@ -1016,6 +1017,11 @@ struct mgpu_plan {
     const volatile long long *d_ctl = nullptr;
     // host staging for run_host
     double *d_y = nullptr;
+    std::vector<int> job_n;           // N of each job, caller order
+    long long *d_job_yoff = nullptr;  // caller-order Y offsets and N, for the matching kernel
+    int *d_job_n = nullptr;
+    int *d_mpairs = nullptr, *d_mcounts = nullptr;
+    int m_cap = 0;
     int *d_nodes = nullptr, *d_status = nullptr, *d_kfail = nullptr;
     size_t y_cap = 0;
     int out_cap = 0;
@@ -1038,6 +1044,8 @@ struct mgpu_plan {
         if (own) cudaStreamDestroy(own);
         for (void *p : allocs) cudaFree(p);
         if (d_y) cudaFree(d_y);
+        if (d_mpairs) cudaFree(d_mpairs);
+        if (d_mcounts) cudaFree(d_mcounts);
         if (d_nodes) cudaFree(d_nodes);
         if (d_status) cudaFree(d_status);
         if (d_kfail) cudaFree(d_kfail);
@@ -1691,8 +1699,17 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         p->vl_smem.push_back(use_vl);
         p->smem.push_back(smem);
     }
+    std::vector<long long> jyoff(njobs);
+    std::vector<int> jn(njobs);
+    for (int j = 0; j < njobs; ++j) {
+        jyoff[j] = (long long)p->yoff[j];
+        jn[j] = systems[job_sys[j]].n;
+    }
+    p->job_n = jn;
     if ((e = upload(p, &p->d_jobs, hj.data(), hj.size())) ||
-        (e = upload(p, &p->d_syslists, syslist.data(), syslist.size()))) {
+        (e = upload(p, &p->d_syslists, syslist.data(), syslist.size())) ||
+        (njobs > 0 && ((e = upload(p, &p->d_job_yoff, jyoff.data(), jyoff.size())) ||
+                       (e = upload(p, &p->d_job_n, jn.data(), jn.size()))))) {
         delete p;
         return set_err(MGPU_ERR_NOMEM, "uploading jobs", e);
     }
@@ -1875,6 +1892,61 @@ int mgpu_plan_run_host(mgpu_plan *p, double *y, int *nodes, int *status, int *kf
         (e = cudaMemcpyAsync(kfail, p->d_kfail, p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)))
         return set_err(MGPU_ERR_CUDA, "copying results to the host", e);
     if ((e = cudaStreamSynchronize(p->own))) return set_err(MGPU_ERR_CUDA, "propagation", e);
+    return MGPU_OK;
+}
+
+int mgpu_plan_match_counts_device(mgpu_plan *p, const double *y_dev, int npairs, const int *pairs_dev,
+                                  int *counts_dev, void *stream)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (npairs < 0) return set_err(MGPU_ERR_ARG, "negative pair count");
+    if (npairs == 0) return MGPU_OK;
+    if (!y_dev || !pairs_dev || !counts_dev) return set_err(MGPU_ERR_ARG, "null device buffer");
+    int nmax = 0;
+    for (int n : p->sys_n) nmax = std::max(nmax, n);
+    if (nmax > match::kMatchMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "device matching counts need N <= 240");
+    const size_t smem = match::packed(nmax, 0) * sizeof(double);
+    cudaError_t e;
+    if ((e = set_smem(match::match_count_kernel, smem))) return set_err(MGPU_ERR_CUDA, "matching kernel set-up", e);
+    for (int b0 = 0; b0 < npairs; b0 += 65535) {
+        const int nb = std::min(65535, npairs - b0);
+        match::match_count_kernel<<<nb, match::kThreads, smem, (cudaStream_t)stream>>>(
+            y_dev, p->d_job_yoff, p->d_job_n, pairs_dev + 2 * (size_t)b0, counts_dev + b0);
+        if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the matching kernel", e);
+    }
+    return MGPU_OK;
+}
+
+int mgpu_plan_match_counts(mgpu_plan *p, int npairs, const int *pairs, int *counts)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (npairs < 0 || (npairs > 0 && (!pairs || !counts))) return set_err(MGPU_ERR_ARG, "bad pair arrays");
+    if (npairs == 0) return MGPU_OK;
+    for (int k = 0; k < 2 * npairs; ++k)
+        if (pairs[k] < 0 || pairs[k] >= p->njobs) return set_err(MGPU_ERR_ARG, "pair references a bad job");
+    for (int k = 0; k < npairs; ++k)
+        if (p->job_n[pairs[2 * k]] != p->job_n[pairs[2 * k + 1]])
+            return set_err(MGPU_ERR_ARG, "paired jobs differ in N");
+    if (!p->d_y || p->y_cap < p->yelems) return set_err(MGPU_ERR_ARG, "no Y on the device: run the plan first");
+    cudaError_t e;
+    if (p->m_cap < npairs) {
+        if (p->d_mpairs) cudaFree(p->d_mpairs);
+        if (p->d_mcounts) cudaFree(p->d_mcounts);
+        p->d_mpairs = p->d_mcounts = nullptr;
+        if ((e = cudaMalloc(&p->d_mpairs, 2 * (size_t)npairs * sizeof(int))) ||
+            (e = cudaMalloc(&p->d_mcounts, (size_t)npairs * sizeof(int))))
+            return set_err(MGPU_ERR_NOMEM, "matching buffers", e);
+        p->m_cap = npairs;
+    }
+    if (!p->own && (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)))
+        return set_err(MGPU_ERR_CUDA, "plan stream", e);
+    if ((e = cudaMemcpyAsync(p->d_mpairs, pairs, 2 * (size_t)npairs * sizeof(int), cudaMemcpyHostToDevice, p->own)))
+        return set_err(MGPU_ERR_CUDA, "copying pairs", e);
+    const int rc = mgpu_plan_match_counts_device(p, p->d_y, npairs, p->d_mpairs, p->d_mcounts, p->own);
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(counts, p->d_mcounts, (size_t)npairs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaStreamSynchronize(p->own)))
+        return set_err(MGPU_ERR_CUDA, "matching counts", e);
     return MGPU_OK;
 }
 

@@ -23,7 +23,7 @@ from typing import Callable
 
 import numpy as np
 
-from .bound import adiabatic_wkb_y, bisect_steps, converge_steps
+from .bound import adiabatic_wkb_y, bisect_steps, converge_steps, matching_counts
 from .propagators import Coupling, Plan, Segment
 
 
@@ -80,10 +80,12 @@ class FieldProblem:
         return adiabatic_wkb_y(c, float(si.rtab[0]), si.ptab[0], e, False)
 
 
-def field_node_counts(fp: FieldProblem, fields) -> tuple:
+def field_node_counts(fp: FieldProblem, fields, eig: bool = True) -> tuple:
     """(counts, NODES_out, NODES_in, matching counts, smallest-magnitude
     matching eigenvalues) at every field, all fields' propagations in one
-    plan."""
+    plan.  eig=False counts the matching matrices' negative eigenvalues on
+    the device (LDL^T inertia; the eigenvalues only where a pivot is zero)
+    and returns NaN for the smallest eigenvalues."""
     fields = np.asarray(fields, dtype=np.float64)
     m = fields.size
     sys_at = [fp.at(float(f)) for f in fields]
@@ -112,12 +114,7 @@ def field_node_counts(fp: FieldProblem, fields) -> tuple:
         else:
             y_in = [plan.unpack(ybuf, m + k) for k in range(m)]
             n_in = nodes[m:].astype(np.int64)
-        nmatch = np.zeros(m, dtype=np.int64)
-        eigmin = np.zeros(m)
-        for k in range(m):
-            ev = np.linalg.eigvalsh(plan.unpack(ybuf, k) - y_in[k])
-            nmatch[k] = int(np.sum(ev <= 0.0))
-            eigmin[k] = ev[np.argmin(np.abs(ev))]
+        nmatch, eigmin = matching_counts(plan, ybuf, y_in, m, eig, host_in)
         n_out = nodes[:m].astype(np.int64)
         return n_out + n_in + nmatch, n_out, n_in, nmatch, eigmin
     finally:
@@ -131,7 +128,7 @@ def find_fields(fp: FieldProblem, fmin: float, fmax: float, tol: float, max_roun
     the crossing where the count of states below the energy steps between k
     and k + 1 (up or down with the field, whichever the end counts say).
     `counter(fp, fields) -> counts` defaults to the GPU node count."""
-    count = counter or (lambda p, f: field_node_counts(p, f)[0])
+    count = counter or (lambda p, f: field_node_counts(p, f, eig=False)[0])
     c0, c1 = (int(x) for x in count(fp, [fmin, fmax]))
     return bisect_steps(lambda xs: count(fp, xs), fmin, fmax, c0, c1, tol, max_rounds)
 

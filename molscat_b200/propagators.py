@@ -282,6 +282,19 @@ class Plan:
         off = int(_lib.load().mgpu_plan_s_offset(self._handle, int(j)))
         return buf[off:off + no * no].reshape((no, no), order="F")
 
+    def match_counts(self, pairs) -> np.ndarray:
+        """After run_host: for each (a, b) job pair, the number of negative
+        eigenvalues of Y_a - Y_b from an LDL^T inertia on the device (the
+        matching count of bdctrl.f:221-257); -1 where a pivot was exactly zero
+        or not finite (count those from the eigenvalues)."""
+        L = _lib.load()
+        pr = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).reshape(-1, 2))
+        out = np.zeros(pr.shape[0], dtype=np.int32)
+        rc = L.mgpu_plan_match_counts(self._handle, pr.shape[0], pr.ctypes.data_as(_ip), out.ctypes.data_as(_ip))
+        if rc != 0:
+            raise PropagatorError(f"matching: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+        return out
+
     def run_host(self, ybuf: np.ndarray):
         """Host buffers in and out.  Returns (Y buffer, NODES, status, kfail)."""
         L = _lib.load()
