@@ -511,6 +511,7 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
     preparations.  The state count at a field is NODES_out + NODES_in + the
     non-positive eigenvalues of Y_out - Y_in; where it changes between
     neighbouring fields a bound state crosses threshold (a resonance field)."""
+    import numpy as np
     import torch
     from molscat_b200.alkali import config4_sweep
     from molscat_b200.propagators import Plan

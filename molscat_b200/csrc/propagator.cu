@@ -1578,7 +1578,9 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         p->sys_nham.push_back(systems[s].nham);
         int owner = s;
         if (kBuckets[b].kind != KIND_BIG) {
-            auto &cand = owners_by_key[std::make_tuple(systems[s].vl, systems[s].iv, grids[s].ptab, grids[s].rtab,
+            // IV is part of the key only where SUMLAM reads it (IVLFL > 0)
+            const int *ivkey = systems[s].ivlfl > 0 ? systems[s].iv : nullptr;
+            auto &cand = owners_by_key[std::make_tuple(systems[s].vl, ivkey, grids[s].ptab, grids[s].rtab,
                                                        systems[s].n, grids[s].nstep, b)];
             for (int r : cand)
                 if (shares_tables(systems[r], grids[r], systems[s], grids[s])) {
