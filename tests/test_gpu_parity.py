@@ -161,6 +161,43 @@ def test_batch_equals_alone():
         plan.close()
 
 
+def _ref_y14(wref, half):
+    """Y14 of the reference-potential solutions (mdprop.f:143-164)."""
+    arg = half * np.sqrt(np.abs(wref))
+    tn, th = np.tan(arg), np.tanh(arg)
+    return np.where(wref < 0.0, arg / tn - arg * tn, arg / th + arg * th)
+
+
+@pytest.mark.parametrize("n", [36, 64, 128, 256])
+@pytest.mark.parametrize("eps", [1e-6, 1e-10])
+def test_tiny_leading_pivot_against_bunch_kaufman(n, eps):
+    """The first matrix MDPROP inverts is made well conditioned (eigenvalues
+    +-1..3) but with a leading diagonal element eps times its largest entry:
+    Bunch-Kaufman (the oracle, as the reference's SYMINL above N = 30) pivots
+    there, the GPU's sweep does not.  The inertia, and so NODES, is the same;
+    the unpivoted inverse loses about u/eps relative accuracy in that one
+    inversion (a host model of the sweep shows 3e-12 at eps 1e-4, 3e-6 at
+    1e-10), which is what the tolerance allows."""
+    from molscat_b200.bound import w_matrix
+    c, seg, ered, _ = cases.random_case(n, 20, seed=4000 + n)
+    h = seg.dr / 2.0
+    d1 = h * h / 3.0
+    w0 = w_matrix(c, float(seg.rtab[0]), seg.ptab[0], ered)
+    wref = np.diag(w_matrix(c, float(seg.rtab[1]), seg.ptab[1], ered))
+    y14b = _ref_y14(wref, 0.5 * h) - d1 * wref
+    rng = np.random.default_rng(n)
+    q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    m = (q * (rng.uniform(1.0, 3.0, n) * rng.choice([-1.0, 1.0], n))) @ q.T
+    m[0, 0] = eps * np.abs(m).max()
+    y0 = (m - d1 * w0 - np.diag(y14b)) / h
+    y0 = 0.5 * (y0 + y0.T)
+    yg, ng = propagate("LDMD", c, seg, ered, y0)
+    yo, no, st, _ = oracle_prop("LDMD", c, seg, ered, y0)
+    assert st == 0
+    assert ng == no
+    assert cases.rel_err(yg, yo) < max(Y_TOL, 100.0 * 1.1e-16 / eps)
+
+
 def test_empty_plan():
     c, seg, ered, y0 = cases.random_case(4, 10, seed=3)
     plan = Plan("LDMD", [c], [seg], np.zeros(0, dtype=np.int32), np.zeros(0))
