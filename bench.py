@@ -521,7 +521,9 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
     cs = [sw.coupling_at(float(f)) for f in fields]
     es = np.array([sw.ered_at(float(f)) for f in fields])
     m = nfield
+    free0, total = torch.cuda.mem_get_info()
     plan = Plan("LDMD", cs + cs, [sw.seg_out] * m + [sw.seg_in] * m, np.arange(2 * m), np.concatenate([es, es]))
+    free1, _ = torch.cuda.mem_get_info()
 
     def starts():
         # adiabatic WKB starts (yinit.f with ADIAMN), all fields in one batched eigh per end
@@ -592,6 +594,7 @@ def field_leg(nfield: int, nout: int, nin: int, reps: int, peak: float | None = 
     work = float(m) * sw.n ** 3 * (nout + nin)
     tfl = plan.flops_prop / (t_prop * 1e-3) / 1e12
     out = {"fields": m, "n": sw.n, "propagations": 2 * m, "shared_systems": plan.shared_systems,
+           "device_gb": {"free_before_plan": free0 / 1e9, "plan": (free0 - free1) / 1e9, "total": total / 1e9},
            "prep_ms": t_prep, "prop_ms": t_prop, "fields_per_s": m / ((t_prep + t_prop) * 1e-3),
            "channel3_steps_per_s": work / ((t_prep + t_prop) * 1e-3), "prop_tflops": tfl,
            "prop_frac": (tfl * 1e12 / peak) if peak else None,
@@ -846,7 +849,13 @@ def main():
             line["large_n"] = large_leg(ns, args.leg_large_energies, args.leg_large_nstep, 2, peak=peak)
             line["large_n"]["peak_source"] = line["roofline"]["peak_source"]
         if not args.no_fields:
-            line["field_sweep"] = field_leg(args.leg_fields, args.leg_field_nout, args.leg_field_nin, 2, peak=peak)
+            try:
+                line["field_sweep"] = field_leg(args.leg_fields, args.leg_field_nout, args.leg_field_nin, 2,
+                                                peak=peak)
+            except Exception as err:  # the headline line is still printed; the leg reports why it failed
+                free, total = torch.cuda.mem_get_info()
+                line["field_sweep"] = {"error": f"{type(err).__name__}: {err}",
+                                       "device_free_gb": free / 1e9, "device_total_gb": total / 1e9}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

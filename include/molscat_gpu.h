@@ -125,7 +125,7 @@ size_t mgpu_plan_y_elems(const mgpu_plan *plan);          /* doubles in a Y buff
 size_t mgpu_plan_y_offset(const mgpu_plan *plan, int job); /* first double of job */
 double mgpu_plan_flops(const mgpu_plan *plan);            /* counted FP64 work (3N^3+2NHAM N(N+1) per step) */
 /* Systems of the plan that use another system's device tables: those that
- * differ from an earlier system (N <= 200) only in EINT and CENT, with the
+ * differ from an earlier system only in EINT and CENT, with the
  * same VL, IV, P and R arrays by address.  They also share its MDPROP U(C)
  * tables and preparation (U uses only the off-diagonal coupling). */
 int mgpu_plan_shared_systems(const mgpu_plan *plan);

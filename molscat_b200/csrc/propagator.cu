@@ -1567,7 +1567,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
     };
     std::vector<SysDev> hs(nsys);
-    // owners by table identity (pointer and scalar key), large-N buckets excluded
+    // owners by table identity (pointer and scalar key)
     std::map<std::tuple<const double *, const int *, const double *, const double *, int, int, int>, std::vector<int>>
         owners_by_key;
     for (int s = 0; s < nsys; ++s) {
@@ -1577,7 +1577,7 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         p->sys_nstep.push_back(grids[s].nstep);
         p->sys_nham.push_back(systems[s].nham);
         int owner = s;
-        if (kBuckets[b].kind != KIND_BIG) {
+        {
             // IV is part of the key only where SUMLAM reads it (IVLFL > 0)
             const int *ivkey = systems[s].ivlfl > 0 ? systems[s].iv : nullptr;
             auto &cand = owners_by_key[std::make_tuple(systems[s].vl, ivkey, grids[s].ptab, grids[s].rtab,

@@ -121,9 +121,24 @@ def test_gpu_field_sweep_counts_match_oracle(gpu, mtot, block, nfield):
 
 
 @pytest.mark.gpu
-def test_gpu_shared_tables_equal_separate(gpu):
+@pytest.mark.parametrize("mtot,block,family", [(8, 1, None), (4, 2, 0), (4, 2, 2)],
+                         ids=["warp-N30", "cta-N106", "big-N106"])
+def test_gpu_shared_tables_equal_separate(gpu, mtot, block, family):
+    """Every kernel family: the one-warp kernels (N = 30), the one-CTA kernels
+    and the batched large-N kernels (N = 106, the family forced)."""
+    from molscat_b200 import _lib
+    if family is not None:
+        _lib.set_family_for_n(97, 112, family, "LDMD")
+    try:
+        _shared_vs_separate(mtot, block)
+    finally:
+        if family is not None:
+            _lib.set_family_for_n(97, 112, -1, "LDMD")
+
+
+def _shared_vs_separate(mtot, block):
     from molscat_b200.propagators import Coupling, Plan, Segment
-    sw = AK.config4_sweep(mtot=8, block=1, nout=300, nin=300)
+    sw = AK.config4_sweep(mtot=mtot, block=block, nout=300, nin=300)
     fields = np.linspace(10.0, 900.0, 6)
     cs = [sw.coupling_at(f) for f in fields]
     es = np.array([sw.ered_at(f) for f in fields])
