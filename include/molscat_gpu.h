@@ -170,8 +170,10 @@ int mgpu_plan_run_device_phases(mgpu_plan *plan, double *y_dev, int *nodes_dev,
  * functions, K from Y by a pivoted linear solve, S = (I + iK)(I - iK)^{-1}.
  * Channels in CHNSRT order (chnsrt.f:16-30: by threshold; the NOPEN open
  * channels first).  S buffers hold, job after job, the NOPEN x NOPEN
- * column-major real (SR) and imaginary (SI) parts.  Every system of the plan
- * must have N <= 64 (else MGPU_ERR_UNSUPPORTED).  A job whose propagation
+ * column-major real (SR) and imaginary (SI) parts.  Up to N = 64 a job's
+ * matrices live in shared memory; up to N = 1024 (every system of the plan,
+ * else MGPU_ERR_UNSUPPORTED) in a device scratch of N(N+NOPEN+1)+NOPEN^2
+ * doubles per job, allocated by the plan on first use.  A job whose propagation
  * failed keeps its status and gets no S; a singular K system sets status to
  * MGPU_ERR_INVERSION. */
 size_t mgpu_plan_s_elems(const mgpu_plan *plan);          /* doubles in an SR (or SI) buffer */

@@ -169,6 +169,178 @@ __device__ int cta_sweep_invert(double *tiles, double *pan, double *xs, double *
     return cnt;
 }
 
+// The same sweep with the tiles held in registers for the whole inversion:
+// warp w owns tiles [w*TPW, (w+1)*TPW) (TPW = ceil(NTL/W), row-major order so
+// a warp's tiles share rows), loaded from shared memory at the start and
+// stored back at the end.  A round then moves only the panel and the
+// operands through shared memory instead of every tile:
+//   0. the owners of tile column K (at and below the diagonal) and of tile
+//      row K (left of it) publish A[i, P] into `pan` as the one-warp sweep
+//      does;                                                      barrier
+//   1. thread i turns its panel row into the operand rows c(i) (B, in place)
+//      and -c(i)/delta (X), rows of P as in cta_sweep_invert;       barrier
+//   2. every warp zeroes row/column block P in its tiles and issues the DMMAs,
+//      the next pivot block's diagonal tile first; its owner gathers that
+//      block with shuffles and factors it (look-ahead);            barrier
+// Per tile the operands, the DMMA and its order are those of
+// cta_sweep_invert, so the result is the same bit for bit.
+template <int NT, int W>
+__device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, double *fbuf, volatile int *cnt_flags,
+                                    int n, const TileRC *tab, int &bad)
+{
+    using C = CG<NT, W>;
+    constexpr int TPW = (C::NTL + W - 1) / W;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int r = lane >> 2, q = lane & 3;
+    const int t0 = warp * TPW;
+    double acc[TPW][2];
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+        const int t = t0 + u;
+        double2 v = make_double2(0.0, 0.0);
+        if (t < C::NTL) v = *reinterpret_cast<const double2 *>(tiles + t * 64 + lane * 2);
+        acc[u][0] = v.x;
+        acc[u][1] = v.y;
+    }
+    // operands of the first block, by warp 0 (shared memory holds the matrix)
+    if (warp == 0) {
+        double f[4][4];
+        load_block4(tiles, 0, f);
+        int c = 0, fl = 0;
+        wf::ldl_block4(f, n, c, fl);
+        if (lane == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) fbuf[i * 4 + j] = f[i][j];
+            cnt_flags[0] = c;
+            cnt_flags[1] = fl;
+        }
+    }
+    __syncthreads();
+    const int nround = (n + 3) >> 2;
+    for (int rd = 0; rd < nround; ++rd) {
+        const int p0 = 4 * rd, K = p0 >> 3, H = (p0 >> 2) & 1;
+        const int p2 = p0 + 4, K2 = p2 >> 3, H2 = (p2 >> 2) & 1;
+        const double *F = fbuf + (rd & 1) * 16;
+        // 0. publish A[i, P] from the lower triangle (row i -> pan[4i .. 4i+3])
+#pragma unroll
+        for (int u = 0; u < TPW; ++u) {
+            const int t = t0 + u;
+            if (t >= C::NTL) break;
+            const int I = tab[t].I, J = tab[t].J;
+            if (J == K && I >= K && (q >> 1) == H && (I > K || H == 0)) {
+                pan[(8 * I + r) * 4 + 2 * q - 4 * H] = acc[u][0];
+                pan[(8 * I + r) * 4 + 2 * q - 4 * H + 1] = acc[u][1];
+            }
+            if (I == K && (r >> 2) == H && (J < K || (J == K && H == 1 && q < 2))) {
+                pan[(8 * J + 2 * q) * 4 + (r & 3)] = acc[u][0];
+                pan[(8 * J + 2 * q + 1) * 4 + (r & 3)] = acc[u][1];
+            }
+        }
+        __syncthreads();
+        // 1. operand rows, in place in pan (B = c) and in xs (X)
+        for (int i = tid; i < C::NPAD; i += C::NTHR) {
+            double c[4], x[4];
+            if (i >= p0 && i < p0 + 4) {
+                const int a = i - p0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const double la = (k == a) ? 1.0 : (k > a ? F[k * 4 + a] : 0.0);
+                    c[k] = -la;
+                    x[k] = la * F[k * 5];
+                }
+            } else {
+                const double2 v01 = *reinterpret_cast<const double2 *>(pan + i * 4);
+                const double2 v23 = *reinterpret_cast<const double2 *>(pan + i * 4 + 2);
+                c[0] = v01.x;
+                c[1] = fma(F[4], v01.x, v01.y);
+                c[2] = fma(F[8], v01.x, fma(F[9], v01.y, v23.x));
+                c[3] = fma(F[12], v01.x, fma(F[13], v01.y, fma(F[14], v23.x, v23.y)));
+#pragma unroll
+                for (int k = 0; k < 4; ++k) x[k] = c[k] * -F[k * 5];
+            }
+            *reinterpret_cast<double2 *>(pan + i * 4) = make_double2(c[0], c[1]);
+            *reinterpret_cast<double2 *>(pan + i * 4 + 2) = make_double2(c[2], c[3]);
+            *reinterpret_cast<double2 *>(xs + i * 4) = make_double2(x[0], x[1]);
+            *reinterpret_cast<double2 *>(xs + i * 4 + 2) = make_double2(x[2], x[3]);
+        }
+        __syncthreads();
+        // 2. trailing update, the next pivot block's diagonal tile first
+        const int tnext = (K2 < NT) ? tix(K2, K2) : -1;
+        const bool own_next = tnext >= t0 && tnext < t0 + TPW;
+#pragma unroll
+        for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+            for (int u = 0; u < TPW; ++u) {
+                const int t = t0 + u;
+                if (t >= C::NTL) break;
+                if ((pass == 0) != (t == tnext)) continue;
+                const int I = tab[t].I, J = tab[t].J;
+                if ((J == K && (q >> 1) == H) || (I == K && (r >> 2) == H)) acc[u][0] = acc[u][1] = 0.0;
+                wf::dmma(acc[u][0], acc[u][1], xs[(8 * I + r) * 4 + q], pan[(8 * J + r) * 4 + q]);
+            }
+            if (pass == 0 && own_next && p2 < n) {
+                // look-ahead: the next block's 4x4 from the tile just updated, by shuffles
+                double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+                for (int u = 0; u < TPW; ++u)
+                    if (t0 + u == tnext) {
+                        v0 = acc[u][0];
+                        v1 = acc[u][1];
+                    }
+                double f[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j <= i; ++j) {
+                        const int src = (4 * H2 + i) * 4 + 2 * H2 + (j >> 1);
+                        const double a0 = __shfl_sync(0xffffffffu, v0, src);
+                        const double a1 = __shfl_sync(0xffffffffu, v1, src);
+                        f[i][j] = (j & 1) ? a1 : a0;
+                    }
+                int c = 0, fl = 0;
+                wf::ldl_block4(f, n - p2, c, fl);
+                if (lane == 0) {
+                    double *Fn = fbuf + ((rd + 1) & 1) * 16;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) Fn[i * 4 + j] = f[i][j];
+                    cnt_flags[0] += c;
+                    cnt_flags[1] |= fl;
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < TPW; ++u) {
+        const int t = t0 + u;
+        if (t < C::NTL) *reinterpret_cast<double2 *>(tiles + t * 64 + lane * 2) = make_double2(acc[u][0], acc[u][1]);
+    }
+    const int cnt = cnt_flags[0];
+    bad = flags_to_status(cnt_flags[1]);
+    __syncthreads();  // every tile is back and the counters are read before they are reused
+    return cnt;
+}
+
+// The sweep the kernels use: tiles in registers (1) or in shared memory (0).
+#ifndef MGPU_CTA_REG
+#define MGPU_CTA_REG 1
+#endif
+template <int NT, int W>
+__device__ __forceinline__ int cta_invert(double *tiles, double *pan, double *xs, double *fbuf, volatile int *cnt_flags,
+                                          int n, const TileRC *tab, int &bad)
+{
+#if MGPU_CTA_REG
+    return cta_sweep_invert_reg<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, tab, bad);
+#else
+    (void)tab;
+    return cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, bad);
+#endif
+}
+
 // W(R) for element x (HAMMAT + SUMLAM), optionally with the diagonal terms.
 __device__ __forceinline__ double w_elem(const SysDev &S, const double *__restrict__ P, int x, int i, int j, int ir,
                                          double ered, bool diag_terms)
@@ -242,7 +414,7 @@ ldmd_prep_cta_kernel(const SysDev *__restrict__ systems, const int *__restrict__
     }
     __syncthreads();
     int bad = SWEEP_OK;
-    const int cnt = cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cf, S.n, bad);
+    const int cnt = cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, S.n, tab, bad);
     if (bad != SWEEP_OK) {
         if (threadIdx.x == 0) {
             atomicMax(&S.prep[1], bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE);
@@ -345,7 +517,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
         }
         __syncthreads();
         int bad = SWEEP_OK;
-        nodes += cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, bad);
+        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, bad);
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -361,7 +533,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
             tiles[x] = v;
         }
         __syncthreads();
-        nodes += cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, bad);
+        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, bad);
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -459,8 +631,8 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
         }
         __syncthreads();
         int bad = SWEEP_OK, bad2 = SWEEP_OK;
-        const int ncu = cta_sweep_invert<NT, W>(ut, pan, xs, fbuf, cf, n, bad);   // ldprop.f:78
-        const int ncz = cta_sweep_invert<NT, W>(zt, pan, xs, fbuf, cf, n, bad2);  // ldprop.f:83
+        const int ncu = cta_invert<NT, W>(ut, pan, xs, fbuf, cf, n, tab, bad);   // ldprop.f:78
+        const int ncz = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, bad2);  // ldprop.f:83
         if (bad != SWEEP_OK || bad2 != SWEEP_OK) {
             status = (bad == SWEEP_ZERO || bad2 == SWEEP_ZERO) ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -473,7 +645,7 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
             zt[x] = -ut[x] + zt[x] - ((i == j && i < n) ? 6.0 : 0.0);  // ldprop.f:92-97
         }
         __syncthreads();
-        const int ncz2 = cta_sweep_invert<NT, W>(zt, pan, xs, fbuf, cf, n, bad);  // ldprop.f:99
+        const int ncz2 = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, bad);  // ldprop.f:99
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;

@@ -1,6 +1,7 @@
 // Y -> K -> S on the device (YTOK/YTOKG/KSYM ytok.f:21-47, ytokg.f:71-126;
-// KTOS ktos.f:149-169), one CTA per propagation, N <= 64 (the matrices live
-// in shared memory).  Included by propagator.cu.
+// KTOS ktos.f:149-169), one CTA per propagation: N <= 64 with the matrices in
+// shared memory, N <= 1024 with them in a global-memory scratch per job (L2
+// resident for the CTAs in flight).  Included by propagator.cu.
 //
 // For channel i with wavevector w_i = sign(E - EINT_i) sqrt|E - EINT_i| and
 // L from CENT_i = L(L+1), at R = the grid's last radius:
@@ -19,10 +20,14 @@
 namespace mgpu {
 namespace smx {
 
-constexpr int kMaxN = 64;
+constexpr int kMaxNShared = 64;  // matrices in shared memory up to here
+constexpr int kMaxN = 1024;       // global-memory scratch above
 constexpr int kThreads = 128;
-// dynamic shared memory: [KM | T] with padded rows, then K
-__host__ __device__ constexpr size_t smem_bytes(int n, int no) { return ((size_t)n * (n + no + 1) + (size_t)no * no) * 8; }
+// the matrices: [KM | T] with padded rows, then K (doubles)
+__host__ __device__ constexpr size_t mat_doubles(int n, int no) { return (size_t)n * (n + no + 1) + (size_t)no * no; }
+__host__ __device__ constexpr size_t smem_bytes(int n, int no) { return mat_doubles(n, no) * 8; }
+// the global-scratch kernel's shared memory: per channel sj, sjp, sn, snp, s_f and the order
+__host__ __device__ constexpr size_t chan_smem_bytes(int n) { return (size_t)n * (5 * 8 + 4); }
 
 struct SJob {
     int sys;         // system index
@@ -32,6 +37,7 @@ struct SJob {
     double ered;
     long long yoff;  // first double of the job's Y
     long long soff;  // first double of the job's SR / SI
+    long long scr;   // first double of the job's matrices in the scratch (N > 64)
 };
 
 // x j_L, (x j_L)', x y_L, (x y_L)'
@@ -156,21 +162,15 @@ __device__ bool gauss_jordan(double *A, int lda, int nr, int ncol, bool pivot, i
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads)
-smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs, const int *__restrict__ nb_all,
-               const int *__restrict__ nb_off, const double *__restrict__ y, double *__restrict__ sr,
-               double *__restrict__ si, int *__restrict__ status)
+// One job: channel functions, [KM | T], Gauss-Jordan, K, then S.  A and K
+// point at shared or global memory; the channel arrays at shared memory.
+__device__ void smatrix_job(const SysDev &S, const SJob &job, const int *__restrict__ nb_all,
+                            const int *__restrict__ nb_off, const double *__restrict__ y, double *__restrict__ sr,
+                            double *__restrict__ si, int *__restrict__ status, double *A, double *K, double *sj,
+                            double *sjp, double *sn, double *snp, double *s_f, int *s_nb, int *s_p)
 {
-    extern __shared__ __align__(16) double smx_sm[];
-    __shared__ double sj[kMaxN], sjp[kMaxN], sn[kMaxN], snp[kMaxN], s_f[kMaxN];
-    __shared__ int s_nb[kMaxN], s_p;
-    const SJob job = jobs[blockIdx.x];
-    const SysDev &S = systems[job.sys];
     const int n = S.n, no = job.nopen, tid = threadIdx.x;
-    if (status[job.out] != MGPU_OK || no == 0) return;  // the propagation failed, or no open channel: no S
     const int lda = n + no + 1;
-    double *A = smx_sm;                      // n x (n + no): [KM | T]
-    double *K = smx_sm + (size_t)n * lda;    // no x no
     const double R = S.rtab[2 * S.nstep];
     for (int c = tid; c < n; c += kThreads) {
         s_nb[c] = nb_all[nb_off[job.sys] + c];
@@ -206,7 +206,7 @@ smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs
         }
     }
     __syncthreads();
-    bool ok = gauss_jordan(A, lda, n, n + no, true, &s_p, s_f);
+    bool ok = gauss_jordan(A, lda, n, n + no, true, s_p, s_f);
     // K = symmetrised open block of KM^{-1} T
     if (ok) {
         for (int e = tid; e < no * no; e += kThreads) {
@@ -228,7 +228,7 @@ smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs
             A[i * lda + j] = v;
         }
         __syncthreads();
-        ok = gauss_jordan(A, lda, no, 2 * no, false, &s_p, s_f);
+        ok = gauss_jordan(A, lda, no, 2 * no, false, s_p, s_f);
     }
     if (!ok) {
         if (tid == 0) status[job.out] = MGPU_ERR_INVERSION;
@@ -244,6 +244,43 @@ smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs
         srj[e] = inv - (i == j ? 1.0 : 0.0);
         sij[e] = v;
     }
+}
+
+// N <= 64: everything in shared memory
+__global__ void __launch_bounds__(kThreads)
+smatrix_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs, const int *__restrict__ nb_all,
+               const int *__restrict__ nb_off, const double *__restrict__ y, double *__restrict__ sr,
+               double *__restrict__ si, int *__restrict__ status)
+{
+    extern __shared__ __align__(16) double smx_sm[];
+    __shared__ double sj[kMaxNShared], sjp[kMaxNShared], sn[kMaxNShared], snp[kMaxNShared], s_f[kMaxNShared];
+    __shared__ int s_nb[kMaxNShared], s_p;
+    const SJob job = jobs[blockIdx.x];
+    const SysDev &S = systems[job.sys];
+    if (status[job.out] != MGPU_OK || job.nopen == 0) return;  // the propagation failed, or no open channel: no S
+    double *A = smx_sm;                                          // n x (n + no): [KM | T]
+    double *K = smx_sm + (size_t)S.n * (S.n + job.nopen + 1);    // no x no
+    smatrix_job(S, job, nb_all, nb_off, y, sr, si, status, A, K, sj, sjp, sn, snp, s_f, s_nb, &s_p);
+}
+
+// N <= 1024: the matrices in the global scratch at job.scr, the channel
+// arrays in shared memory (chan_smem_bytes)
+__global__ void __launch_bounds__(kThreads)
+smatrix_kernel_g(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs, const int *__restrict__ nb_all,
+                 const int *__restrict__ nb_off, const double *__restrict__ y, double *__restrict__ sr,
+                 double *__restrict__ si, int *__restrict__ status, double *__restrict__ scratch)
+{
+    extern __shared__ __align__(16) double smx_sm[];
+    __shared__ int s_p;
+    const SJob job = jobs[blockIdx.x];
+    const SysDev &S = systems[job.sys];
+    if (status[job.out] != MGPU_OK || job.nopen == 0) return;
+    const int n = S.n;
+    double *sj = smx_sm, *sjp = sj + n, *sn = sjp + n, *snp = sn + n, *s_f = snp + n;
+    int *s_nb = reinterpret_cast<int *>(s_f + n);
+    double *A = scratch + job.scr;
+    double *K = A + (size_t)n * (n + job.nopen + 1);
+    smatrix_job(S, job, nb_all, nb_off, y, sr, si, status, A, K, sj, sjp, sn, snp, s_f, s_nb, &s_p);
 }
 
 }  // namespace smx

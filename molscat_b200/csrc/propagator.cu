@@ -992,13 +992,17 @@ struct mgpu_plan {
     std::vector<int> bucket_ids, job_begin, job_count, sys_begin, sys_count, max_nstep, vl_smem;
     std::vector<size_t> smem;
     std::vector<BigBucket> big;            // large-N buckets (KIND_BIG)
-    // Y -> S on the device (every system N <= 64): channel order NB per system, NOPEN and S offsets per job
+    // Y -> S on the device (every system N <= 1024): channel order NB per system, NOPEN and S offsets per job;
+    // jobs with N <= 64 in shared memory (d_sjobs), the others with their matrices in a global scratch
     bool s_ok = false;
     std::vector<int> nopen;
     std::vector<size_t> soff;
     size_t selems = 0;
-    size_t s_smem = 0;
-    smx::SJob *d_sjobs = nullptr;
+    size_t s_smem = 0, s_smem_g = 0;
+    int ns_small = 0, ns_large = 0;
+    size_t sscr_elems = 0;
+    double *d_sscr = nullptr;
+    smx::SJob *d_sjobs = nullptr, *d_sjobs_g = nullptr;
     int *d_nb = nullptr, *d_nb_off = nullptr;
     double *d_sr = nullptr, *d_si = nullptr;
     size_t s_cap = 0;
@@ -1044,6 +1048,7 @@ struct mgpu_plan {
         if (own) cudaStreamDestroy(own);
         for (void *p : allocs) cudaFree(p);
         if (d_y) cudaFree(d_y);
+        if (d_sscr) cudaFree(d_sscr);
         if (d_mpairs) cudaFree(d_mpairs);
         if (d_mcounts) cudaFree(d_mcounts);
         if (d_nodes) cudaFree(d_nodes);
@@ -1769,8 +1774,8 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
                 }
             nb_all.insert(nb_all.end(), nb.begin(), nb.end());
         }
-        std::vector<smx::SJob> sj(njobs);
-        size_t so = 0;
+        std::vector<smx::SJob> sj, sjg;
+        size_t so = 0, scr = 0;
         for (int j = 0; j < njobs; ++j) {
             const mgpu_coupling &c = systems[job_sys[j]];
             int no = 0;
@@ -1778,19 +1783,36 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
             p->nopen[j] = no;
             p->soff[j] = so;
             so += (size_t)no * no;
-            sj[j].sys = job_sys[j];
-            sj[j].nopen = no;
-            sj[j].out = j;
-            sj[j].pad = 0;
-            sj[j].ered = job_ered[j];
-            sj[j].yoff = (long long)p->yoff[j];
-            sj[j].soff = (long long)p->soff[j];
-            p->s_smem = std::max(p->s_smem, smx::smem_bytes(c.n, no));
+            smx::SJob q;
+            q.sys = job_sys[j];
+            q.nopen = no;
+            q.out = j;
+            q.pad = 0;
+            q.ered = job_ered[j];
+            q.yoff = (long long)p->yoff[j];
+            q.soff = (long long)p->soff[j];
+            q.scr = 0;
+            if (c.n <= smx::kMaxNShared) {
+                p->s_smem = std::max(p->s_smem, smx::smem_bytes(c.n, no));
+                sj.push_back(q);
+            } else {
+                if (no > 0) {
+                    q.scr = (long long)scr;
+                    scr += smx::mat_doubles(c.n, no);
+                }
+                p->s_smem_g = std::max(p->s_smem_g, smx::chan_smem_bytes(c.n));
+                sjg.push_back(q);
+            }
         }
         p->selems = so;
+        p->sscr_elems = scr;
+        p->ns_small = (int)sj.size();
+        p->ns_large = (int)sjg.size();
         p->s_ok = ok;
         if (ok && njobs > 0 &&
-            ((e = upload(p, &p->d_sjobs, sj.data(), sj.size())) || (e = upload(p, &p->d_nb, nb_all.data(), nb_all.size())) ||
+            ((!sj.empty() && (e = upload(p, &p->d_sjobs, sj.data(), sj.size()))) ||
+             (!sjg.empty() && (e = upload(p, &p->d_sjobs_g, sjg.data(), sjg.size()))) ||
+             (e = upload(p, &p->d_nb, nb_all.data(), nb_all.size())) ||
              (e = upload(p, &p->d_nb_off, nb_off.data(), nb_off.size())))) {
             delete p;
             return set_err(MGPU_ERR_NOMEM, "uploading S-matrix descriptors", e);
@@ -1965,14 +1987,28 @@ int mgpu_plan_smatrix_device(mgpu_plan *p, const double *y_dev, double *sr_dev, 
                              void *stream)
 {
     if (!p) return set_err(MGPU_ERR_ARG, "null plan");
-    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 64 in every system");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 1024 in every system");
     if (p->njobs == 0 || p->selems == 0) return MGPU_OK;
     if (!y_dev || !sr_dev || !si_dev || !status_dev) return set_err(MGPU_ERR_ARG, "null device buffer");
     cudaError_t e;
-    if ((e = set_smem(smx::smatrix_kernel, p->s_smem))) return set_err(MGPU_ERR_CUDA, "S-matrix kernel set-up", e);
-    smx::smatrix_kernel<<<p->njobs, smx::kThreads, p->s_smem, (cudaStream_t)stream>>>(
-        p->d_sys, p->d_sjobs, p->d_nb, p->d_nb_off, y_dev, sr_dev, si_dev, status_dev);
-    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the S-matrix kernel", e);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (int j0 = 0; j0 < p->ns_small; j0 += 65535) {
+        if ((e = set_smem(smx::smatrix_kernel, p->s_smem))) return set_err(MGPU_ERR_CUDA, "S-matrix kernel set-up", e);
+        smx::smatrix_kernel<<<std::min(65535, p->ns_small - j0), smx::kThreads, p->s_smem, st>>>(
+            p->d_sys, p->d_sjobs + j0, p->d_nb, p->d_nb_off, y_dev, sr_dev, si_dev, status_dev);
+        if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the S-matrix kernel", e);
+    }
+    if (p->ns_large > 0) {
+        if (!p->d_sscr && p->sscr_elems > 0 && (e = cudaMalloc(&p->d_sscr, p->sscr_elems * sizeof(double))))
+            return set_err(MGPU_ERR_NOMEM, "S-matrix scratch", e);
+        if ((e = set_smem(smx::smatrix_kernel_g, p->s_smem_g)))
+            return set_err(MGPU_ERR_CUDA, "S-matrix kernel set-up", e);
+        for (int j0 = 0; j0 < p->ns_large; j0 += 65535) {
+            smx::smatrix_kernel_g<<<std::min(65535, p->ns_large - j0), smx::kThreads, p->s_smem_g, st>>>(
+                p->d_sys, p->d_sjobs_g + j0, p->d_nb, p->d_nb_off, y_dev, sr_dev, si_dev, status_dev, p->d_sscr);
+            if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the S-matrix kernel", e);
+        }
+    }
     return MGPU_OK;
 }
 
@@ -1980,7 +2016,7 @@ int mgpu_plan_run_host_smatrix(mgpu_plan *p, const double *y, double *sr, double
                                int *kfail)
 {
     if (!p) return set_err(MGPU_ERR_ARG, "null plan");
-    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 64 in every system");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 1024 in every system");
     if (p->njobs == 0) return MGPU_OK;
     if (!y || !nodes || !status || !kfail || (p->selems && (!sr || !si))) return set_err(MGPU_ERR_ARG, "null host buffer");
     cudaError_t e;

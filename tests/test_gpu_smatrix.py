@@ -1,5 +1,6 @@
 """Y -> K -> S on the device (YTOK/YTOKG/KSYM + KTOS) against the oracle's
-restatement and the reference's printed S matrices (absolute 1e-8)."""
+restatement and the reference's printed S matrices (absolute 1e-8), up to
+N = 1024 (matrices in shared memory to N = 64, in a device scratch above)."""
 import numpy as np
 import pytest
 
@@ -84,10 +85,44 @@ def test_rotor_smatrix_on_device_equals_oracle(jtot, block):
     plan.close()
 
 
-def test_smatrix_needs_small_n():
-    c, seg, ered, y0 = cases.random_case(70, 10, seed=5)
-    plan = Plan("LDMD", [c], [seg], np.zeros(1, dtype=np.int32), np.array([ered]))
+@pytest.mark.parametrize("ns", [(70,), (100, 36), (200,), (300, 130)])
+def test_smatrix_large_n_on_device_equals_oracle(ns):
+    """N above 64 (matrices in the device scratch), mixed with N <= 64 jobs
+    in one plan: S against YTOK/KTOS on the device's own Y, per job, every
+    energy with open and closed channels."""
+    systems, segs, job_sys, job_e, y0s = [], [], [], [], []
+    for s, n in enumerate(ns):
+        c, seg, ered, y0 = cases.random_case(n, 40, seed=600 + n)
+        systems.append(c)
+        segs.append(seg)
+        for de in (0.0, 7.0):
+            job_sys.append(s)
+            job_e.append(ered + de)
+            y0s.append(y0)
+    plan = Plan("LDMD", systems, segs, np.array(job_sys, dtype=np.int32), np.array(job_e))
+    ybuf, nodes, status, _ = plan.run_host(plan.pack(y0s))
+    sr, si, nodes2, status2, _ = plan.run_host_smatrix(plan.pack(y0s))
+    assert (status == 0).all() and (status2 == 0).all()
+    assert np.array_equal(nodes, nodes2)
+    for j in range(plan.njobs):
+        c, seg = systems[job_sys[j]], segs[job_sys[j]]
+        so_r, so_i = oracle_s(c, seg, job_e[j], plan.unpack(ybuf, j))
+        assert plan.nopen(j) == so_r.shape[0] and so_r.size > 0
+        err = max(np.abs(plan.unpack_s(sr, j) - so_r).max(), np.abs(plan.unpack_s(si, j) - so_i).max())
+        assert err < S_TOL, (j, err)
+        sm = plan.unpack_s(sr, j) + 1j * plan.unpack_s(si, j)
+        assert np.abs(sm @ sm.conj().T - np.eye(sm.shape[0])).max() < 1e-9
+    plan.close()
+
+
+def test_smatrix_needs_n_up_to_1024():
+    c, seg, ered, y0 = cases.random_case(1100, 2, seed=5)
     from molscat_b200.propagators import PropagatorError
+    try:
+        plan = Plan("LDMD", [c], [seg], np.zeros(1, dtype=np.int32), np.array([ered]))
+    except PropagatorError as e:  # the propagation's own limit
+        assert e.status == _lib.MGPU_ERR_UNSUPPORTED
+        return
     with pytest.raises(PropagatorError) as e:
         plan.run_host_smatrix(plan.pack([y0]))
     assert e.value.status == _lib.MGPU_ERR_UNSUPPORTED
