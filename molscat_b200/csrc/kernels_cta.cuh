@@ -325,20 +325,23 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, doub
     return cnt;
 }
 
-// The sweep the kernels use: tiles in registers (1) or in shared memory (0).
-#ifndef MGPU_CTA_REG
-#define MGPU_CTA_REG 1
+// The sweep the kernels use: tiles in registers from NT = MGPU_CTA_REG_NT up
+// (N > 104: 1.2x at N = 106, 1.9x at 150, 2.1x at 200 on B200), in shared
+// memory below it (where more CTAs per SM win: 0.76x / 0.90x at N = 48 / 72
+// with the tiles in registers).  Both give the same result bit for bit.
+#ifndef MGPU_CTA_REG_NT
+#define MGPU_CTA_REG_NT 14
 #endif
 template <int NT, int W>
 __device__ __forceinline__ int cta_invert(double *tiles, double *pan, double *xs, double *fbuf, volatile int *cnt_flags,
                                           int n, const TileRC *tab, int &bad)
 {
-#if MGPU_CTA_REG
-    return cta_sweep_invert_reg<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, tab, bad);
-#else
-    (void)tab;
-    return cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, bad);
-#endif
+    if constexpr (NT >= MGPU_CTA_REG_NT) {
+        return cta_sweep_invert_reg<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, tab, bad);
+    } else {
+        (void)tab;
+        return cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, bad);
+    }
 }
 
 // W(R) for element x (HAMMAT + SUMLAM), optionally with the diagonal terms.

@@ -147,7 +147,7 @@ __device__ bool gauss_jordan(double *A, int lda, int nr, int ncol, bool pivot, i
         if (piv == 0.0 || !isfinite(piv)) return false;
         const double rp = 1.0 / piv;
         for (int j = k + 1 + tid; j < ncol; j += kThreads) A[k * lda + j] *= rp;
-        if (tid < nr) s_f[tid] = A[tid * lda + k];
+        for (int i = tid; i < nr; i += kThreads) s_f[i] = A[i * lda + k];
         __syncthreads();
         if (tid == 0) A[k * lda + k] = 1.0;
         const int w = ncol - k - 1;
