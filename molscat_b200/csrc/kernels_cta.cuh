@@ -36,7 +36,12 @@ struct CG {
 template <int NT, int W>
 struct CSmem {
     static constexpr int PAN = CG<NT, W>::NPAD * 4;
-    static size_t bytes(int nmat) { return (size_t)(nmat * CG<NT, W>::TD + 2 * PAN + 32 + 3 * CG<NT, W>::NPAD) * 8; }
+    // the second panel / operand pair of the register-resident sweep, after the rest
+    __host__ __device__ static constexpr size_t extra(int nmat)
+    {
+        return (size_t)nmat * CG<NT, W>::TD + 2 * PAN + 32 + 3 * CG<NT, W>::NPAD;
+    }
+    __host__ __device__ static constexpr size_t bytes(int nmat) { return (extra(nmat) + 2 * PAN) * 8; }
 };
 
 struct TileRC {
@@ -169,6 +174,12 @@ __device__ int cta_sweep_invert(double *tiles, double *pan, double *xs, double *
     return cnt;
 }
 
+// 1: the register-resident sweep alternates two panel / operand buffers and
+// drops the round's closing barrier; 0: one buffer, three barriers a round.
+#ifndef MGPU_CTA_DB
+#define MGPU_CTA_DB 1
+#endif
+
 // The same sweep with the tiles held in registers for the whole inversion:
 // warp w owns tiles [w*TPW, (w+1)*TPW) (TPW = ceil(NTL/W), row-major order so
 // a warp's tiles share rows), loaded from shared memory at the start and
@@ -185,8 +196,8 @@ __device__ int cta_sweep_invert(double *tiles, double *pan, double *xs, double *
 // Per tile the operands, the DMMA and its order are those of
 // cta_sweep_invert, so the result is the same bit for bit.
 template <int NT, int W>
-__device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, double *fbuf, volatile int *cnt_flags,
-                                    int n, const TileRC *tab, int &bad)
+__device__ int cta_sweep_invert_reg(double *tiles, double *pan0, double *xs0, double *fbuf, volatile int *cnt_flags,
+                                    int n, const TileRC *tab, double *pan1, int &bad)
 {
     using C = CG<NT, W>;
     constexpr int TPW = (C::NTL + W - 1) / W;
@@ -223,6 +234,16 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, doub
         const int p0 = 4 * rd, K = p0 >> 3, H = (p0 >> 2) & 1;
         const int p2 = p0 + 4, K2 = p2 >> 3, H2 = (p2 >> 2) & 1;
         const double *F = fbuf + (rd & 1) * 16;
+#if MGPU_CTA_DB
+        // alternate panel / operand buffers: a round's publication cannot
+        // overwrite what a slower warp still reads in the previous round's
+        // DMMAs, so the round needs no closing barrier
+        double *pan = (rd & 1) ? pan1 : pan0;
+        double *xs = (rd & 1) ? pan1 + CSmem<NT, W>::PAN : xs0;
+#else
+        double *pan = pan0;
+        double *xs = xs0;
+#endif
         // 0. publish A[i, P] from the lower triangle (row i -> pan[4i .. 4i+3])
 #pragma unroll
         for (int u = 0; u < TPW; ++u) {
@@ -312,8 +333,13 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, doub
                 }
             }
         }
+#if !MGPU_CTA_DB
         __syncthreads();
+#endif
     }
+#if MGPU_CTA_DB
+    __syncthreads();  // the last round's look-ahead counters are in
+#endif
 #pragma unroll
     for (int u = 0; u < TPW; ++u) {
         const int t = t0 + u;
@@ -326,20 +352,22 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan, double *xs, doub
 }
 
 // The sweep the kernels use: tiles in registers from NT = MGPU_CTA_REG_NT up
-// (N > 104: 1.2x at N = 106, 1.9x at 150, 2.1x at 200 on B200), in shared
-// memory below it (where more CTAs per SM win: 0.76x / 0.90x at N = 48 / 72
-// with the tiles in registers).  Both give the same result bit for bit.
+// (N > 80: 1.1x at N = 96, 1.3x at 106, 2.1x at 150 and 200 on B200, double
+// buffered), in shared memory below it (where more CTAs per SM make up for
+// it: 0.76x at N = 48, equal at 72 with the tiles in registers).  Both give
+// the same result bit for bit.
 #ifndef MGPU_CTA_REG_NT
-#define MGPU_CTA_REG_NT 14
+#define MGPU_CTA_REG_NT 12
 #endif
 template <int NT, int W>
 __device__ __forceinline__ int cta_invert(double *tiles, double *pan, double *xs, double *fbuf, volatile int *cnt_flags,
-                                          int n, const TileRC *tab, int &bad)
+                                          int n, const TileRC *tab, double *extra, int &bad)
 {
     if constexpr (NT >= MGPU_CTA_REG_NT) {
-        return cta_sweep_invert_reg<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, tab, bad);
+        return cta_sweep_invert_reg<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, tab, extra, bad);
     } else {
         (void)tab;
+        (void)extra;
         return cta_sweep_invert<NT, W>(tiles, pan, xs, fbuf, cnt_flags, n, bad);
     }
 }
@@ -417,7 +445,7 @@ ldmd_prep_cta_kernel(const SysDev *__restrict__ systems, const int *__restrict__
     }
     __syncthreads();
     int bad = SWEEP_OK;
-    const int cnt = cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, S.n, tab, bad);
+    const int cnt = cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, S.n, tab, sm + CSmem<NT, W>::extra(1), bad);
     if (bad != SWEEP_OK) {
         if (threadIdx.x == 0) {
             atomicMax(&S.prep[1], bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE);
@@ -520,7 +548,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
         }
         __syncthreads();
         int bad = SWEEP_OK;
-        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, bad);
+        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(1), bad);
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -536,7 +564,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
             tiles[x] = v;
         }
         __syncthreads();
-        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, bad);
+        nodes += cta_invert<NT, W>(tiles, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(1), bad);
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -634,8 +662,8 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
         }
         __syncthreads();
         int bad = SWEEP_OK, bad2 = SWEEP_OK;
-        const int ncu = cta_invert<NT, W>(ut, pan, xs, fbuf, cf, n, tab, bad);   // ldprop.f:78
-        const int ncz = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, bad2);  // ldprop.f:83
+        const int ncu = cta_invert<NT, W>(ut, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(2), bad);   // ldprop.f:78
+        const int ncz = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(2), bad2);  // ldprop.f:83
         if (bad != SWEEP_OK || bad2 != SWEEP_OK) {
             status = (bad == SWEEP_ZERO || bad2 == SWEEP_ZERO) ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
@@ -648,7 +676,7 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
             zt[x] = -ut[x] + zt[x] - ((i == j && i < n) ? 6.0 : 0.0);  // ldprop.f:92-97
         }
         __syncthreads();
-        const int ncz2 = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, bad);  // ldprop.f:99
+        const int ncz2 = cta_invert<NT, W>(zt, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(2), bad);  // ldprop.f:99
         if (bad != SWEEP_OK) {
             status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
             kfail = k;
