@@ -193,7 +193,9 @@ int mgpu_plan_run_host_smatrix(mgpu_plan *plan, const double *y, double *sr, dou
  * a failed inversion; the large-N kernels run their steps to the end.
  * mgpu_plan_cancel(plan, 1): runs in progress and later runs stop with
  *   MGPU_ERR_CANCELLED (callable from any host thread while a run is in
- *   flight: the controls live in mapped host memory); (plan, 0) clears it.
+ *   flight: the controls live in device memory and are written by a copy
+ *   on a stream of their own, which the copy engine serves beside running
+ *   kernels; the call returns once the copy has landed); (plan, 0) clears it.
  * mgpu_plan_set_time_limit(plan, s): a step kernel that has run longer than s
  *   seconds (the device's global timer, from that kernel's start) stops its
  *   jobs with MGPU_ERR_DEADLINE; 0 removes the limit. */

@@ -244,20 +244,25 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan0, double *xs0, do
         double *pan = pan0;
         double *xs = xs0;
 #endif
-        // 0. publish A[i, P] from the lower triangle (row i -> pan[4i .. 4i+3])
+        // 0. publish A[i, P] from the lower triangle (row i -> pan[4i .. 4i+3]),
+        //    then zero row / column block P in the tiles that hold it (tile
+        //    row and tile column K, the only ones with entries there)
 #pragma unroll
         for (int u = 0; u < TPW; ++u) {
             const int t = t0 + u;
             if (t >= C::NTL) break;
-            const int I = tab[t].I, J = tab[t].J;
-            if (J == K && I >= K && (q >> 1) == H && (I > K || H == 0)) {
+            const TileRC ij = tab[t];
+            const int I = ij.I, J = ij.J;
+            if (I != K && J != K) continue;
+            if (J == K && (q >> 1) == H && (I > K || H == 0)) {
                 pan[(8 * I + r) * 4 + 2 * q - 4 * H] = acc[u][0];
                 pan[(8 * I + r) * 4 + 2 * q - 4 * H + 1] = acc[u][1];
             }
-            if (I == K && (r >> 2) == H && (J < K || (J == K && H == 1 && q < 2))) {
+            if (I == K && (r >> 2) == H && (J < K || (H == 1 && q < 2))) {
                 pan[(8 * J + 2 * q) * 4 + (r & 3)] = acc[u][0];
                 pan[(8 * J + 2 * q + 1) * 4 + (r & 3)] = acc[u][1];
             }
+            if ((J == K && (q >> 1) == H) || (I == K && (r >> 2) == H)) acc[u][0] = acc[u][1] = 0.0;
         }
         __syncthreads();
         // 1. operand rows, in place in pan (B = c) and in xs (X)
@@ -289,17 +294,19 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan0, double *xs0, do
         __syncthreads();
         // 2. trailing update, the next pivot block's diagonal tile first
         const int tnext = (K2 < NT) ? tix(K2, K2) : -1;
-        const bool own_next = tnext >= t0 && tnext < t0 + TPW;
+        const int unext = tnext - t0;  // in [0, TPW) for the warp that owns it
+        const bool own_next = unext >= 0 && unext < TPW;
+        const double *xr = xs + r * 4 + q;   // X_I = xr[32 I], B_J = br[32 J]
+        const double *br = pan + r * 4 + q;
 #pragma unroll
         for (int pass = 0; pass < 2; ++pass) {
 #pragma unroll
             for (int u = 0; u < TPW; ++u) {
+                if ((pass == 0) != (u == unext)) continue;
                 const int t = t0 + u;
                 if (t >= C::NTL) break;
-                if ((pass == 0) != (t == tnext)) continue;
-                const int I = tab[t].I, J = tab[t].J;
-                if ((J == K && (q >> 1) == H) || (I == K && (r >> 2) == H)) acc[u][0] = acc[u][1] = 0.0;
-                wf::dmma(acc[u][0], acc[u][1], xs[(8 * I + r) * 4 + q], pan[(8 * J + r) * 4 + q]);
+                const TileRC ij = tab[t];
+                wf::dmma(acc[u][0], acc[u][1], xr[32 * ij.I], br[32 * ij.J]);
             }
             if (pass == 0 && own_next && p2 < n) {
                 // look-ahead: the next block's 4x4 from the tile just updated, by shuffles

@@ -46,7 +46,7 @@ struct SysDev {
     const double *ptab; // [2*nstep+1][nham]
     double *q;          // LDMD: [nstep][T*T][ntiles] 2HQ(C_k)
     int *prep;          // LDMD: [0] negative pivots of all U inversions (NSAVE), [1] status, [2] kfail
-    const volatile long long *ctl;  // plan's stop controls (mapped host memory) or null: stop_requested
+    const volatile long long *ctl;  // plan's stop controls (device memory) or null: stop_requested
 };
 
 struct JobDev {
@@ -1016,9 +1016,14 @@ struct mgpu_plan {
     std::vector<BigStreams> bstreams;
     cudaStream_t own = nullptr;            // run_host's copies and launches
     cudaEvent_t ev_in = nullptr;
-    // stop controls the step kernels poll: [0] cancel, [1] time budget (ns), mapped host memory
-    volatile long long *ctl = nullptr;
-    const volatile long long *d_ctl = nullptr;
+    // stop controls the step kernels poll: [0] cancel, [1] time budget (ns).
+    // They live in device memory (a poll is an L2 read, not a PCIe round
+    // trip from every warp); the host writes them from a pinned mirror on a
+    // stream of their own, which the copy engine serves while kernels run.
+    long long *ctl = nullptr;            // pinned host mirror
+    long long *d_ctl = nullptr;
+    cudaStream_t ctl_stream = nullptr;
+    std::mutex ctl_mu;
     // host staging for run_host
     double *d_y = nullptr;
     std::vector<int> job_n;           // N of each job, caller order
@@ -1057,6 +1062,8 @@ struct mgpu_plan {
         if (d_sr) cudaFree(d_sr);
         if (d_si) cudaFree(d_si);
         if (ctl) cudaFreeHost((void *)ctl);
+        if (d_ctl) cudaFree(d_ctl);
+        if (ctl_stream) cudaStreamDestroy(ctl_stream);
     }
     template <class X>
     cudaError_t dalloc(X **p, size_t count)
@@ -1441,12 +1448,25 @@ int mgpu_probe_fp64_fma(double *out_dev, int iters, void *stream, double *flops_
     return MGPU_OK;
 }
 
+// Write the stop controls to the device: from the pinned mirror, on the
+// controls' own stream (served by the copy engine beside running kernels),
+// waited for before returning.
+static int push_ctl(mgpu_plan *plan)
+{
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(plan->d_ctl, plan->ctl, 2 * sizeof(long long), cudaMemcpyHostToDevice,
+                             plan->ctl_stream)) ||
+        (e = cudaStreamSynchronize(plan->ctl_stream)))
+        return set_err(MGPU_ERR_CUDA, "writing the stop controls", e);
+    return MGPU_OK;
+}
+
 int mgpu_plan_cancel(mgpu_plan *plan, int on)
 {
     if (!plan || !plan->ctl) return set_err(MGPU_ERR_ARG, "null plan");
+    std::lock_guard<std::mutex> lk(plan->ctl_mu);
     plan->ctl[0] = on ? 1 : 0;
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    return MGPU_OK;
+    return push_ctl(plan);
 }
 
 int mgpu_plan_set_time_limit(mgpu_plan *plan, double seconds)
@@ -1454,9 +1474,9 @@ int mgpu_plan_set_time_limit(mgpu_plan *plan, double seconds)
     if (!plan || !plan->ctl) return set_err(MGPU_ERR_ARG, "null plan");
     if (!(seconds >= 0.0) || !std::isfinite(seconds)) return set_err(MGPU_ERR_ARG, "time limit must be >= 0");
     const double ns = seconds * 1.0e9;
+    std::lock_guard<std::mutex> lk(plan->ctl_mu);
     plan->ctl[1] = (seconds == 0.0) ? 0 : (ns < 1.0 ? 1 : (ns > 9.0e18 ? (long long)9e18 : (long long)ns));
-    std::atomic_thread_fence(std::memory_order_seq_cst);
-    return MGPU_OK;
+    return push_ctl(plan);
 }
 
 int mgpu_set_step_wait_limit(int limit)
@@ -1632,17 +1652,20 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     }
     for (int s = 0; s < nsys; ++s) hs[s].prep = p->d_prep + 3 * p->sys_owner[s];
     {
-        void *h = nullptr, *dptr = nullptr;
-        if ((e = cudaHostAlloc(&h, 2 * sizeof(long long), cudaHostAllocMapped)) ||
-            (e = cudaHostGetDevicePointer(&dptr, h, 0))) {
-            if (h) cudaFreeHost(h);
+        void *h = nullptr;
+        if ((e = cudaHostAlloc(&h, 2 * sizeof(long long), cudaHostAllocDefault))) {
             delete p;
             return set_err(MGPU_ERR_NOMEM, "allocating the stop controls", e);
         }
-        p->ctl = static_cast<volatile long long *>(h);
+        p->ctl = static_cast<long long *>(h);
         p->ctl[0] = 0;
         p->ctl[1] = 0;
-        p->d_ctl = static_cast<const volatile long long *>(dptr);
+        if ((e = cudaStreamCreateWithFlags(&p->ctl_stream, cudaStreamNonBlocking)) ||
+            (e = p->dalloc(&p->d_ctl, 2)) ||
+            (e = cudaMemcpy(p->d_ctl, p->ctl, 2 * sizeof(long long), cudaMemcpyHostToDevice))) {
+            delete p;
+            return set_err(MGPU_ERR_NOMEM, "allocating the stop controls", e);
+        }
     }
     for (int s = 0; s < nsys; ++s) hs[s].ctl = p->d_ctl;
     if ((e = upload(p, &p->d_sys, hs.data(), hs.size()))) {

@@ -313,11 +313,16 @@ __device__ uint32_t g_step_wait_limit = kWaitLimit;
 
 // A stop the host asks for, polled by the step kernels every kStopPoll steps
 // (k = 1, 1 + kStopPoll, ...): ctl points at the plan's control words in
-// mapped host memory, ctl[0] != 0 cancels, ctl[1] > 0 is each step kernel's
+// device memory (volatile reads: L2, where the host's copies land; reading
+// them from mapped host memory cost every warp a PCIe round trip and the
+// batched workload 24 %), ctl[0] != 0 cancels, ctl[1] > 0 is each step kernel's
 // time budget in nanoseconds on the device's global timer, counted from that
 // kernel's start.  The kernel then records the status and the step and
 // leaves its loop as it does after a failed inversion.
-constexpr int kStopPoll = 128;
+#ifndef MGPU_STOP_POLL
+#define MGPU_STOP_POLL 128
+#endif
+constexpr int kStopPoll = MGPU_STOP_POLL;
 
 __device__ __forceinline__ unsigned long long global_ns()
 {
