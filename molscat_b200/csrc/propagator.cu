@@ -1061,8 +1061,7 @@ struct mgpu_plan {
         if (d_kfail) cudaFree(d_kfail);
         if (d_sr) cudaFree(d_sr);
         if (d_si) cudaFree(d_si);
-        if (ctl) cudaFreeHost((void *)ctl);
-        if (d_ctl) cudaFree(d_ctl);
+        if (ctl) cudaFreeHost((void *)ctl);  // d_ctl is one of `allocs`
         if (ctl_stream) cudaStreamDestroy(ctl_stream);
     }
     template <class X>
