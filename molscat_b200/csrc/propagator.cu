@@ -624,7 +624,9 @@ __global__ void __launch_bounds__(256) pivot_reciprocal_probe_kernel(const doubl
 #define MGPU_BUCKETS(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(12) X(14) X(16)
 #define MGPU_FRAG_BUCKETS(X) X(1) X(2) X(3) X(4) X(5)
 // (NT, warps) of the one-CTA-per-matrix buckets, N = 8*NT up to 200
+#ifndef MGPU_CTA_BUCKETS
 #define MGPU_CTA_BUCKETS(X) X(6, 4) X(7, 4) X(8, 4) X(10, 8) X(12, 8) X(14, 8) X(16, 8) X(20, 16) X(25, 16)
+#endif
 
 // NT of the large-N buckets (matrices in global memory, 64 pivots a round):
 // N up to 1024 in steps of 64
