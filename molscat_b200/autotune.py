@@ -12,6 +12,10 @@ range's largest N, many energies) and keeps the fastest:
 
     python -m molscat_b200.autotune [--prop LDMD] [--out molscat_b200/tuning/ldmd.json]
 
+One family at one N, timed once (the case a profiler capture is taken on):
+
+    python -m molscat_b200.autotune --one 106 --family 0 --jobs 1024 --nstep 50
+
 `apply(path)` hands the saved choices to the library
 (mgpu_set_family_for_n); plans created afterwards use them.
 """
@@ -115,9 +119,18 @@ def main():
     ap.add_argument("--prop", default="LDMD", choices=["LDMD", "LDJ"])
     ap.add_argument("--out", default=None)
     ap.add_argument("--nstep", type=int, default=100)
+    ap.add_argument("--one", type=int, default=0, help="time one family at this N and print TFLOP/s")
+    ap.add_argument("--family", type=int, default=_lib.FAMILY_DMMA)
+    ap.add_argument("--jobs", type=int, default=1024)
     a = ap.parse_args()
     from .build import build
     build()
+    if a.one:
+        tf = measure(a.one, a.prop, a.family, a.jobs, a.nstep)
+        print(json.dumps({"n": a.one, "family": a.family, "jobs": a.jobs, "nstep": a.nstep, "tflops": tf}))
+        if tf <= 0.0:
+            raise SystemExit("propagation reported a non-zero status")
+        return
     t = tune(a.prop, nstep=a.nstep)
     out = a.out or default_path(a.prop)
     os.makedirs(os.path.dirname(out), exist_ok=True)

@@ -41,7 +41,8 @@ struct CSmem {
     {
         return (size_t)nmat * CG<NT, W>::TD + 2 * PAN + 32 + 3 * CG<NT, W>::NPAD;
     }
-    __host__ __device__ static constexpr size_t bytes(int nmat) { return (extra(nmat) + 2 * PAN) * 8; }
+    // + 32 doubles of slack: a padding tile's operand reads run up to 31 past the last buffer
+    __host__ __device__ static constexpr size_t bytes(int nmat) { return (extra(nmat) + 2 * PAN + 32) * 8; }
 };
 
 struct TileRC {
@@ -249,9 +250,7 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan0, double *xs0, do
         //    row and tile column K, the only ones with entries there)
 #pragma unroll
         for (int u = 0; u < TPW; ++u) {
-            const int t = t0 + u;
-            if (t >= C::NTL) break;
-            const TileRC ij = tab[t];
+            const TileRC ij = tab[t0 + u];
             const int I = ij.I, J = ij.J;
             if (I != K && J != K) continue;
             if (J == K && (q >> 1) == H && (I > K || H == 0)) {
@@ -298,17 +297,20 @@ __device__ int cta_sweep_invert_reg(double *tiles, double *pan0, double *xs0, do
         const bool own_next = unext >= 0 && unext < TPW;
         const double *xr = xs + r * 4 + q;   // X_I = xr[32 I], B_J = br[32 J]
         const double *br = pan + r * 4 + q;
+        // (tab has W*TPW entries; those past NTL name a tile beyond the matrix
+        // whose operand reads stay inside shared memory and whose result is
+        // never stored, so the loops need no bound test)
 #pragma unroll
         for (int pass = 0; pass < 2; ++pass) {
 #pragma unroll
             for (int u = 0; u < TPW; ++u) {
                 if ((pass == 0) != (u == unext)) continue;
-                const int t = t0 + u;
-                if (t >= C::NTL) break;
-                const TileRC ij = tab[t];
+                const TileRC ij = tab[t0 + u];
                 wf::dmma(acc[u][0], acc[u][1], xr[32 * ij.I], br[32 * ij.J]);
             }
-            if (pass == 0 && own_next && p2 < n) {
+            // the look-ahead after this warp's other DMMAs are issued, so they
+            // run while it factors
+            if (pass == 1 && own_next && p2 < n) {
                 // look-ahead: the next block's 4x4 from the tile just updated, by shuffles
                 double v0 = 0.0, v1 = 0.0;
 #pragma unroll
@@ -407,10 +409,19 @@ __device__ __forceinline__ double w_elem(const SysDev &S, const double *__restri
     return w;
 }
 
+// Tile t -> (I, J); entries from NTL up to the padded count tabn<NT, W>()
+// name (NT, NT), a tile beyond the matrix (see cta_sweep_invert_reg).
+template <int NT, int W>
+__host__ __device__ constexpr int tabn() { return W * ((CG<NT, W>::NTL + W - 1) / W); }
+
 template <int NT, int W>
 __device__ __forceinline__ void build_table(TileRC *tab)
 {
-    for (int t = threadIdx.x; t < CG<NT, W>::NTL; t += CG<NT, W>::NTHR) {
+    for (int t = threadIdx.x; t < tabn<NT, W>(); t += CG<NT, W>::NTHR) {
+        if (t >= CG<NT, W>::NTL) {
+            tab[t].I = tab[t].J = (unsigned char)NT;
+            continue;
+        }
         int I = 0;
         while ((I + 1) * (I + 2) / 2 <= t) ++I;
         tab[t].I = (unsigned char)I;
@@ -427,7 +438,7 @@ ldmd_prep_cta_kernel(const SysDev *__restrict__ systems, const int *__restrict__
 {
     using C = CG<NT, W>;
     extern __shared__ __align__(16) double sm[];
-    __shared__ TileRC tab[C::NTL];
+    __shared__ TileRC tab[tabn<NT, W>()];
     __shared__ int cf[2];
     __shared__ SysDev s_sys;
     if (threadIdx.x == 0) s_sys = systems[sys_list[blockIdx.y]];
@@ -480,7 +491,7 @@ ldmd_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
 {
     using C = CG<NT, W>;
     extern __shared__ __align__(16) double sm[];
-    __shared__ TileRC tab[C::NTL];
+    __shared__ TileRC tab[tabn<NT, W>()];
     __shared__ int cf[2];
     __shared__ int s_stop;
     __shared__ SysDev s_sys;
@@ -618,7 +629,7 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
 {
     using C = CG<NT, W>;
     extern __shared__ __align__(16) double sm[];
-    __shared__ TileRC tab[C::NTL];
+    __shared__ TileRC tab[tabn<NT, W>()];
     __shared__ int cf[2];
     __shared__ int s_stop;
     __shared__ SysDev s_sys;
