@@ -809,8 +809,9 @@ def main():
             "config": {"workload": "rotor close-coupling (ITYPE=1 style) MDPROP: JTOT=0..%d x 2 parities x %d energies "
                                    "(1-500 cm-1), 4000 steps 2.5-40 A, N=5..36" % (args.jmax, args.energies),
                        "systems": len(wl.systems), "propagations_per_gpu": njobs,
-                       "l2": "inputs larger than L2 (2HQ(C) tables %.1f GB)" % (plan.flops_prep and
-                                                                                 sum(16 * (((s.n + 3) // 4) * ((s.n + 3) // 4 + 1) // 2) * 8 * 4000 for s in wl.systems) / 1e9),
+                       "l2": "inputs larger than L2 (2HQ(C) and coupling-sum tables %.1f GB)" % (
+                           2 * sum(512 * (((s.n + 7) // 8) * ((s.n + 7) // 8 + 1) // 2) * 4000 for s in wl.systems)
+                           / 1e9),
                        "parallelism": ("LPT shards of (block, 512 energies) units over %d GPUs, no collective on the "
                                        "data path" % world) if world > 1 else "1 GPU",
                        "tuning": f"molscat_b200/tuning/ldmd.json ({tuned} N ranges off the default family)"},

@@ -23,10 +23,11 @@ struct WarpSmem {
     static constexpr size_t BYTES = (size_t)DOUBLES * 8;
 };
 
-// W(R) on this lane's fragment (HAMMAT + SUMLAM, hammat.f:85-113).
+// The coupling sum sum_l VL_l P_l(R_ir) on this lane's fragment (SUMLAM,
+// sumlam.f:29-36,74-86): the part of W(R) that does not depend on the
+// energy or on EINT/CENT.
 template <int NT>
-__device__ __forceinline__ void w_frag(const SysDev &S, int lane, int ir, double ered, bool diag_terms,
-                                       double (&w)[G<NT>::NTL][2])
+__device__ __forceinline__ void w_sum_frag(const SysDev &S, int lane, int ir, double (&w)[G<NT>::NTL][2])
 {
     constexpr int NTL = G<NT>::NTL;
     const double *P = S.ptab + (size_t)ir * S.nham;
@@ -53,34 +54,78 @@ __device__ __forceinline__ void w_frag(const SysDev &S, int lane, int ir, double
                 }
         }
     }
-    if (diag_terms) {
-        const double R = __ldg(S.rtab + ir);
-        const double rsq = fmin(1.0 / (R * R), 1.0e16);
-        double conf = 0.0;
-        if (S.conlen > 0.0) {
-            const double c2 = S.conlen * S.conlen;
-            conf = R * R / (c2 * c2);
-        }
-        const int r = lane >> 2, q = lane & 3;
-#pragma unroll
-        for (int I = 0; I < NT; ++I)
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-                const int i = 8 * I + r;
-                if (r == 2 * q + s && i < S.n) {
-                    double x = w[tix(I, I)][s];
-                    if (S.nrsq == 0) x += rsq * S.cent[i];
-                    if (S.nconst == 0) x += S.eint[i];
-                    if (S.conlen > 0.0) x += conf;
-                    w[tix(I, I)][s] = x - ered;
-                }
-            }
+}
+
+// The diagonal terms of W(R_ir) (HAMMAT, hammat.f:85-113): CENT/R^2 (the
+// 1e16 clamp), EINT, the confinement term, then -ERED.  x is the coupling
+// sum of channel i's diagonal element.
+__device__ __forceinline__ double w_diag_terms(const SysDev &S, int i, double x, double rsq, double conf, double ered)
+{
+    if (S.nrsq == 0) x += rsq * S.cent[i];
+    if (S.nconst == 0) x += S.eint[i];
+    if (S.conlen > 0.0) x += conf;
+    return x - ered;
+}
+
+__device__ __forceinline__ void w_radial(const SysDev &S, int ir, double &rsq, double &conf)
+{
+    const double R = __ldg(S.rtab + ir);
+    rsq = fmin(1.0 / (R * R), 1.0e16);
+    conf = 0.0;
+    if (S.conlen > 0.0) {
+        const double c2 = S.conlen * S.conlen;
+        conf = R * R / (c2 * c2);
     }
 }
 
-// W(R)_ii (the DIAG array of HAMMAT) for channel i.
 template <int NT>
-__device__ __forceinline__ double w_diag_frag(const SysDev &S, int i, int ir, double ered)
+__device__ __forceinline__ void w_diag_frag_terms(const SysDev &S, int lane, int ir, double ered,
+                                                  double (&w)[G<NT>::NTL][2])
+{
+    double rsq, conf;
+    w_radial(S, ir, rsq, conf);
+    const int r = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int I = 0; I < NT; ++I)
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int i = 8 * I + r;
+            if (r == 2 * q + s && i < S.n) w[tix(I, I)][s] = w_diag_terms(S, i, w[tix(I, I)][s], rsq, conf, ered);
+        }
+}
+
+// W(R) on this lane's fragment (HAMMAT + SUMLAM, hammat.f:85-113).
+template <int NT>
+__device__ __forceinline__ void w_frag(const SysDev &S, int lane, int ir, double ered, bool diag_terms,
+                                       double (&w)[G<NT>::NTL][2])
+{
+    w_sum_frag<NT>(S, lane, ir, w);
+    if (diag_terms) w_diag_frag_terms<NT>(S, lane, ir, ered, w);
+}
+
+// W(R_2m) for the step loop: the coupling sum from the system's table when
+// it has one (the preparation wrote it), else from VL; then the diagonal.
+template <int NT>
+__device__ __forceinline__ void w_step_frag(const SysDev &S, int lane, int m, double ered, double (&w)[G<NT>::NTL][2])
+{
+    constexpr int NTL = G<NT>::NTL;
+    if (S.wt != nullptr) {
+        const double *src = S.wt + (size_t)m * NTL * 64 + lane * 2;
+#pragma unroll
+        for (int t = 0; t < NTL; ++t) {
+            const double2 x = __ldg(reinterpret_cast<const double2 *>(src + t * 64));
+            w[t][0] = x.x;
+            w[t][1] = x.y;
+        }
+    } else {
+        w_sum_frag<NT>(S, lane, 2 * m, w);
+    }
+    w_diag_frag_terms<NT>(S, lane, 2 * m, ered, w);
+}
+
+// The coupling sum of W(R_ir)_ii for channel i.
+template <int NT>
+__device__ __forceinline__ double w_diag_sum_frag(const SysDev &S, int i, int ir)
 {
     constexpr int NTL = G<NT>::NTL;
     const int I = i >> 3, r = i & 7;
@@ -93,15 +138,28 @@ __device__ __forceinline__ double w_diag_frag(const SysDev &S, int i, int ir, do
         if (S.ivlfl <= 0) x = fma(v, __ldg(P + l), x);
         else if (v != 0.0) x = fma(v, __ldg(P + __ldg(S.ivt + (size_t)l * NTL * 64 + e)), x);
     }
-    const double R = __ldg(S.rtab + ir);
-    const double rsq = fmin(1.0 / (R * R), 1.0e16);
-    if (S.nrsq == 0) x += rsq * S.cent[i];
-    if (S.nconst == 0) x += S.eint[i];
-    if (S.conlen > 0.0) {
-        const double c2 = S.conlen * S.conlen;
-        x += R * R / (c2 * c2);
-    }
-    return x - ered;
+    return x;
+}
+
+// W(R)_ii (the DIAG array of HAMMAT) for channel i.
+template <int NT>
+__device__ __forceinline__ double w_diag_frag(const SysDev &S, int i, int ir, double ered)
+{
+    double rsq, conf;
+    w_radial(S, ir, rsq, conf);
+    return w_diag_terms(S, i, w_diag_sum_frag<NT>(S, i, ir), rsq, conf, ered);
+}
+
+// W(R_2k-1)_ii for the step loop, the coupling sum from the system's table
+// when it has one.
+template <int NT>
+__device__ __forceinline__ double w_mid_diag_frag(const SysDev &S, int i, int k, double ered)
+{
+    double rsq, conf;
+    w_radial(S, 2 * k - 1, rsq, conf);
+    const double x = S.wd != nullptr ? __ldg(S.wd + (size_t)(k - 1) * G<NT>::NPAD + i)
+                                     : w_diag_sum_frag<NT>(S, i, 2 * k - 1);
+    return w_diag_terms(S, i, x, rsq, conf, ered);
 }
 
 template <int NT>
@@ -159,7 +217,26 @@ ldmd_prep_frag_kernel(const SysDev *__restrict__ systems, const int *__restrict_
     const double d1 = h * h / 3.0;
     const double d4 = -d1 / 16.0;
     double a[NTL][2];
-    w_frag<NT>(S, lane, 2 * k - 1, 0.0, false, a);
+    if (S.wt != nullptr) {
+        // the step loop's coupling sums: W at R_2k (and R_0 for the first
+        // step) and the diagonal at R_2k-1, the same arithmetic as there
+        for (int m = (k == 1 ? 0 : k); m <= k; ++m) {
+            w_sum_frag<NT>(S, lane, 2 * m, a);
+            double *dst = S.wt + (size_t)m * NTL * 64 + lane * 2;
+#pragma unroll
+            for (int t = 0; t < NTL; ++t)
+                *reinterpret_cast<double2 *>(dst + t * 64) = make_double2(a[t][0], a[t][1]);
+        }
+    }
+    w_sum_frag<NT>(S, lane, 2 * k - 1, a);
+    if (S.wd != nullptr) {
+        const int r = lane >> 2, q = lane & 3;
+#pragma unroll
+        for (int I = 0; I < NT; ++I)
+#pragma unroll
+            for (int s = 0; s < 2; ++s)
+                if (r == 2 * q + s) S.wd[(size_t)(k - 1) * G<NT>::NPAD + 8 * I + r] = a[tix(I, I)][s];
+    }
 #pragma unroll
     for (int I = 0; I < NT; ++I)
 #pragma unroll
@@ -256,7 +333,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
     {
         double w[NTL][2];
         load_lower_frag<NT>(yj, n, lane, a);
-        w_frag<NT>(S, lane, 0, ered, true, w);
+        w_step_frag<NT>(S, lane, 0, ered, w);
 #pragma unroll
         for (int t = 0; t < NTL; ++t)
 #pragma unroll
@@ -280,7 +357,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
         // reference-potential solutions in the sector (mdprop.f:143-164)
         __syncwarp();
         for (int i = lane; i < n; i += 32) {
-            const double wref = w_diag_frag<NT>(S, i, 2 * k - 1, ered);
+            const double wref = w_mid_diag_frag<NT>(S, i, k, ered);
             double y14, y23;
             ref_solutions(wref, half, y14, y23);
             s_y14[i] = y14;
@@ -347,7 +424,7 @@ ldmd_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restri
         {
             const double dd = (k == nstep) ? d1 : d2;
             double w[NTL][2];
-            w_frag<NT>(S, lane, 2 * k, ered, true, w);
+            w_step_frag<NT>(S, lane, k, ered, w);
 #pragma unroll
             for (int I = 0; I < NT; ++I)
 #pragma unroll

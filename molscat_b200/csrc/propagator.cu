@@ -45,6 +45,9 @@ struct SysDev {
     const double *rtab; // [2*nstep+1]
     const double *ptab; // [2*nstep+1][nham]
     double *q;          // LDMD: [nstep][T*T][ntiles] 2HQ(C_k)
+    double *wt;         // LDMD one-warp kernels or null: [nstep+1][ntiles][64] coupling sum
+                        // sum_l VL_l P_l(R) at R_0, R_2, .., R_2nstep (fragment layout)
+    double *wd;         // LDMD one-warp kernels or null: [nstep][npad] its diagonal at R_1, R_3, ..
     int *prep;          // LDMD: [0] negative pivots of all U inversions (NSAVE), [1] status, [2] kfail
     const volatile long long *ctl;  // plan's stop controls (device memory) or null: stop_requested
 };
@@ -1187,6 +1190,10 @@ static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, i
         return set_err(MGPU_ERR_NOMEM, "uploading a system", e);
     if (iprop == MGPU_PROP_LDMD && (e = alloc_n(al, &dq, (size_t)g.nstep * TT * nt)))
         return set_err(MGPU_ERR_NOMEM, "allocating the 2HQ(C) table", e);
+    double *dwt = nullptr, *dwd = nullptr;
+    if (iprop == MGPU_PROP_LDMD && kBuckets[b].kind == KIND_FRAG8 &&
+        ((e = alloc_n(al, &dwt, ((size_t)g.nstep + 1) * TT * nt)) || (e = alloc_n(al, &dwd, (size_t)g.nstep * npad))))
+        return set_err(MGPU_ERR_NOMEM, "allocating the coupling-sum tables", e);
     d.vlt = dv;
     d.ivt = di;
     d.eint = de;
@@ -1194,6 +1201,8 @@ static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, i
     d.rtab = drt;
     d.ptab = dpt;
     d.q = dq;
+    d.wt = dwt;
+    d.wd = dwd;
     d.ctl = nullptr;
     return MGPU_OK;
 }
