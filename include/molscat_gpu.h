@@ -186,6 +186,29 @@ int mgpu_plan_smatrix_device(mgpu_plan *plan, const double *y_dev, double *sr_de
 int mgpu_plan_run_host_smatrix(mgpu_plan *plan, const double *y, double *sr, double *si, int *nodes,
                                int *status, int *kfail);
 
+/* YTRANS (ytrans.f90:1-485) before YTOK: system `sys`'s Y -> S inputs from
+ * now on are the asymptotic basis EVEC (n x n column-major; its columns the
+ * asymptotic channels, the eigenvectors of the asymptotic Hamiltonian block
+ * by block, as YTRANS leaves them in EVEC) or NULL (Y already in that
+ * basis), the thresholds EINT[n] and L(L+1) values CENT[n] of those
+ * channels (YTRANS's EINT and CENT on exit), and the matching radius RMATCH
+ * (the reference's RMAX when a long-range segment follows the plan's grid).
+ * The device transforms Y' = EVEC^T Y EVEC (TRNSFM, ytrans.f90:410-413)
+ * into a buffer of the plan's own and runs YTOK/KTOS on Y'; CHNSRT order,
+ * NOPEN and the S offsets follow the new thresholds (mgpu_plan_nopen,
+ * mgpu_plan_s_offset and mgpu_plan_s_elems change accordingly).  The
+ * propagation is not affected: it keeps the coupling's EINT and CENT.  The
+ * asymptotic Hamiltonian and its diagonalisation stay on the host (they do
+ * not depend on the energy: once per system). */
+int mgpu_plan_set_asymptote(mgpu_plan *plan, int sys, const double *eint, const double *cent,
+                            const double *evec, double rmatch);
+/* Y -> K -> S alone, from host matrices (the jobs' Y at their matching
+ * radius, in the plan's Y layout): status[njobs] in (the propagations'
+ * statuses; a job with a non-zero status gets no S) and out (as
+ * mgpu_plan_smatrix_device leaves it).  For a long-range segment that ran
+ * elsewhere between the plan's propagation and the matching. */
+int mgpu_plan_smatrix_host(mgpu_plan *plan, const double *y, double *sr, double *si, int *status);
+
 /* Stopping a plan's runs from the host.  The step kernels of the one-warp,
  * one-CTA and 4x4-tile families (N <= 200; LDPROP <= 128) poll the plan's
  * controls every 128 steps (steps 1, 129, 257, ...) and a job that sees a

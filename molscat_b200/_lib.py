@@ -51,7 +51,8 @@ EXPORTS = (
     "mgpu_server_create", "mgpu_server_destroy", "mgpu_server_add_system", "mgpu_submit", "mgpu_poll",
     "mgpu_wait", "mgpu_request_times", "mgpu_release", "mgpu_server_in_flight", "mgpu_set_family_for_n",
     "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
-    "mgpu_plan_run_host_smatrix", "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
+    "mgpu_plan_run_host_smatrix", "mgpu_plan_set_asymptote", "mgpu_plan_smatrix_host",
+    "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
     "mgpu_plan_cancel", "mgpu_plan_set_time_limit", "mgpu_set_step_wait_limit",
 )
 
@@ -112,6 +113,8 @@ def load(path: str | None = None):
     L.mgpu_plan_nopen.argtypes = [vp, ctypes.c_int]
     L.mgpu_plan_smatrix_device.argtypes = [vp, vp, vp, vp, vp, vp]
     L.mgpu_plan_run_host_smatrix.argtypes = [vp, _dp, _dp, _dp, _ip, _ip, _ip]
+    L.mgpu_plan_set_asymptote.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
+    L.mgpu_plan_smatrix_host.argtypes = [vp, _dp, _dp, _dp, _ip]
     ll = ctypes.c_longlong
     L.mgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]

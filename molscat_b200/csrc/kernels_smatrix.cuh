@@ -4,7 +4,9 @@
 // resident for the CTAs in flight).  Included by propagator.cu.
 //
 // For channel i with wavevector w_i = sign(E - EINT_i) sqrt|E - EINT_i| and
-// L from CENT_i = L(L+1), at R = the grid's last radius:
+// L from CENT_i = L(L+1), at the matching radius R (the grid's last radius
+// unless the caller set another, with YTRANS's thresholds where it set an
+// asymptotic basis):
 //   open   (E > EINT):  sj = x j_L(x)/sqrt(w), sjp = (x j_L)'(x) sqrt(w),
 //                       sn = x y_L(x)/sqrt(w), snp = (x y_L)'(x) sqrt(w),  x = w R
 //   closed:             sn = 1, snp = |w| d/dx ln[x k_L(x)],  x = |w| R
@@ -38,6 +40,10 @@ struct SJob {
     long long yoff;  // first double of the job's Y
     long long soff;  // first double of the job's SR / SI
     long long scr;   // first double of the job's matrices in the scratch (N > 64)
+    const double *eint;  // [n] thresholds: the coupling's EINT, or YTRANS's asymptotic ones
+    const double *cent;  // [n] L(L+1)
+    const double *evec;  // [n*n] column-major asymptotic basis, or null (Y already in it)
+    double rmatch;       // R of the matching: the grid's last radius unless set
 };
 
 // x j_L, (x j_L)', x y_L, (x y_L)'
@@ -171,12 +177,12 @@ __device__ void smatrix_job(const SysDev &S, const SJob &job, const int *__restr
 {
     const int n = S.n, no = job.nopen, tid = threadIdx.x;
     const int lda = n + no + 1;
-    const double R = S.rtab[2 * S.nstep];
+    const double R = job.rmatch;
     for (int c = tid; c < n; c += kThreads) {
         s_nb[c] = nb_all[nb_off[job.sys] + c];
-        const double dif = job.ered - S.eint[c];
+        const double dif = job.ered - job.eint[c];
         const double w = copysign(sqrt(fabs(dif)), dif);
-        const int ell = (int)lrint(sqrt(S.cent[c] + 0.25) - 0.5);
+        const int ell = (int)lrint(sqrt(job.cent[c] + 0.25) - 0.5);
         if (dif > 0.0) {
             double uj, ujp, un, unp;
             riccati(ell, w * R, uj, ujp, un, unp);
@@ -281,6 +287,63 @@ smatrix_kernel_g(const SysDev *__restrict__ systems, const SJob *__restrict__ jo
     double *A = scratch + job.scr;
     double *K = A + (size_t)n * (n + job.nopen + 1);
     smatrix_job(S, job, nb_all, nb_off, y, sr, si, status, A, K, sj, sjp, sn, snp, s_f, s_nb, &s_p);
+}
+
+// YTRANS's transform (TRNSFM, ytrans.f90:410-413) Y' = EVEC^T Y EVEC for
+// the jobs whose system has an asymptotic basis, as two products of 32x32
+// output tiles (pass 1: Z = Y EVEC; pass 2: Y' = EVEC^T Z); a job without
+// one is copied by pass 2.  grid (ceil(nmax/32)^2, jobs); 256 threads, each
+// four outputs of the tile's column.
+constexpr int kTT = 32;
+__global__ void __launch_bounds__(256)
+ytrans_kernel(const SysDev *__restrict__ systems, const SJob *__restrict__ jobs, int pass,
+              const double *__restrict__ y, double *__restrict__ z, double *__restrict__ yt)
+{
+    __shared__ double As[kTT][kTT + 1], Bs[kTT][kTT + 1];
+    const SJob job = jobs[blockIdx.y];
+    const int n = systems[job.sys].n;
+    const int tilesx = (n + kTT - 1) / kTT;
+    const int ti = (int)blockIdx.x % tilesx, tj = (int)blockIdx.x / tilesx;
+    if (tj >= tilesx) return;  // the grid covers the largest n
+    const int i0 = ti * kTT, j0 = tj * kTT, t = threadIdx.x;
+    const int tc = t & 31, tr = t >> 5;
+    const double *T = job.evec;
+    const double *A = pass == 1 ? y + job.yoff : T;   // pass 1: Y;  pass 2: EVEC (read transposed)
+    const double *B = pass == 1 ? T : z + job.yoff;    // pass 1: EVEC; pass 2: Z
+    double *C = (pass == 1 ? z : yt) + job.yoff;
+    if (T == nullptr) {
+        if (pass == 1) return;
+        for (int e = t; e < kTT * kTT; e += 256) {
+            const int r = e & 31, c = e >> 5;
+            if (i0 + r < n && j0 + c < n) C[(i0 + r) + (size_t)(j0 + c) * n] = y[job.yoff + (i0 + r) + (size_t)(j0 + c) * n];
+        }
+        return;
+    }
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k0 = 0; k0 < n; k0 += kTT) {
+        for (int e = t; e < kTT * kTT; e += 256) {
+            const int f = e & 31, g = e >> 5;
+            if (pass == 1) {  // As[r][k] = Y(i0 + r, k0 + k), r fastest
+                As[f][g] = (i0 + f < n && k0 + g < n) ? A[(i0 + f) + (size_t)(k0 + g) * n] : 0.0;
+            } else {          // As[r][k] = EVEC(k0 + k, i0 + r), k fastest
+                As[g][f] = (i0 + g < n && k0 + f < n) ? A[(k0 + f) + (size_t)(i0 + g) * n] : 0.0;
+            }
+            Bs[f][g] = (k0 + f < n && j0 + g < n) ? B[(k0 + f) + (size_t)(j0 + g) * n] : 0.0;  // Bs[k][c]
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int k = 0; k < kTT; ++k) {
+            const double b = Bs[k][tc];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[u] = fma(As[tr + 8 * u][k], b, acc[u]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int r = tr + 8 * u;
+        if (i0 + r < n && j0 + tc < n) C[(i0 + r) + (size_t)(j0 + tc) * n] = acc[u];
+    }
 }
 
 }  // namespace smx

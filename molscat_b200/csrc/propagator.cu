@@ -1011,6 +1011,17 @@ struct mgpu_plan {
     int *d_nb = nullptr, *d_nb_off = nullptr;
     double *d_sr = nullptr, *d_si = nullptr;
     size_t s_cap = 0;
+    // per-system inputs of Y -> S: thresholds and L(L+1) (host copies for the
+    // channel order, device pointers for the kernels), the matching radius,
+    // and YTRANS's asymptotic basis where the caller set one
+    std::vector<std::vector<double>> s_eint;
+    std::vector<const double *> s_deint, s_dcent, s_devec;
+    std::vector<double> s_rmatch;
+    std::vector<int> job_sys;
+    std::vector<double> job_ered;
+    int n_evec = 0;                        // systems with an asymptotic basis
+    double *d_yz = nullptr, *d_yt = nullptr;  // the transform's product and result (yelems each)
+    int sn_max = 0;
     // Streams of the large-N buckets: each bucket's step loop runs on its own
     // stream (never the legacy stream: graph capture) with a high-priority
     // look-ahead stream beside it, so buckets of different N overlap on the GPU.
@@ -1066,8 +1077,20 @@ struct mgpu_plan {
         if (d_kfail) cudaFree(d_kfail);
         if (d_sr) cudaFree(d_sr);
         if (d_si) cudaFree(d_si);
+        if (d_yz) cudaFree(d_yz);
+        if (d_yt) cudaFree(d_yt);
         if (ctl) cudaFreeHost((void *)ctl);  // d_ctl is one of `allocs`
         if (ctl_stream) cudaStreamDestroy(ctl_stream);
+    }
+    void dfree(void *q)
+    {
+        if (!q) return;
+        for (auto it = allocs.begin(); it != allocs.end(); ++it)
+            if (*it == q) {
+                allocs.erase(it);
+                break;
+            }
+        cudaFree(q);
     }
     template <class X>
     cudaError_t dalloc(X **p, size_t count)
@@ -1568,6 +1591,90 @@ int mgpu_plan_launches(const mgpu_plan *p)
     return l;
 }
 
+// The S-matrix descriptors from the plan's per-system S inputs: channel
+// order (CHNSRT, chnsrt.f:16-30: by threshold, equal thresholds within
+// 1e-11 keep their order), open channels and S offsets per job; jobs with
+// N <= 64 in shared memory, the others with their matrices in a scratch.
+static int build_s(mgpu_plan *p)
+{
+    const int nsys = p->nsys, njobs = p->njobs;
+    std::vector<int> nb_all, nb_off(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        const std::vector<double> &ei = p->s_eint[s];
+        const int n = (int)ei.size();
+        nb_off[s] = (int)nb_all.size();
+        std::vector<int> nb(n);
+        for (int i = 0; i < n; ++i) nb[i] = i;
+        for (int i = 0; i + 1 < n; ++i)
+            for (int j = i + 1; j < n; ++j) {
+                const double a = ei[nb[i]], bb = ei[nb[j]];
+                if (a <= bb || std::fabs(a - bb) < 1.0e-11) continue;
+                std::swap(nb[i], nb[j]);
+            }
+        nb_all.insert(nb_all.end(), nb.begin(), nb.end());
+    }
+    std::vector<smx::SJob> sj, sjg;
+    p->nopen.assign(njobs, 0);
+    p->soff.assign(njobs, 0);
+    p->s_smem = p->s_smem_g = 0;
+    size_t so = 0, scr = 0;
+    for (int j = 0; j < njobs; ++j) {
+        const int sy = p->job_sys[j];
+        const std::vector<double> &ei = p->s_eint[sy];
+        const int n = (int)ei.size();
+        int no = 0;
+        for (int i = 0; i < n; ++i) no += (p->job_ered[j] - ei[i] > 0.0) ? 1 : 0;
+        p->nopen[j] = no;
+        p->soff[j] = so;
+        so += (size_t)no * no;
+        smx::SJob q;
+        q.sys = sy;
+        q.nopen = no;
+        q.out = j;
+        q.pad = 0;
+        q.ered = p->job_ered[j];
+        q.yoff = (long long)p->yoff[j];
+        q.soff = (long long)p->soff[j];
+        q.scr = 0;
+        q.eint = p->s_deint[sy];
+        q.cent = p->s_dcent[sy];
+        q.evec = p->s_devec[sy];
+        q.rmatch = p->s_rmatch[sy];
+        if (n <= smx::kMaxNShared) {
+            p->s_smem = std::max(p->s_smem, smx::smem_bytes(n, no));
+            sj.push_back(q);
+        } else {
+            if (no > 0) {
+                q.scr = (long long)scr;
+                scr += smx::mat_doubles(n, no);
+            }
+            p->s_smem_g = std::max(p->s_smem_g, smx::chan_smem_bytes(n));
+            sjg.push_back(q);
+        }
+    }
+    p->selems = so;
+    if (scr != p->sscr_elems && p->d_sscr) {
+        cudaFree(p->d_sscr);
+        p->d_sscr = nullptr;
+    }
+    p->sscr_elems = scr;
+    p->ns_small = (int)sj.size();
+    p->ns_large = (int)sjg.size();
+    p->dfree(p->d_sjobs);
+    p->dfree(p->d_sjobs_g);
+    p->dfree(p->d_nb);
+    p->dfree(p->d_nb_off);
+    p->d_sjobs = p->d_sjobs_g = nullptr;
+    p->d_nb = p->d_nb_off = nullptr;
+    cudaError_t e;
+    if (njobs > 0 && ((!sj.empty() && (e = upload(p, &p->d_sjobs, sj.data(), sj.size()))) ||
+                      (!sjg.empty() && (e = upload(p, &p->d_sjobs_g, sjg.data(), sjg.size()))) ||
+                      (e = upload(p, &p->d_nb, nb_all.data(), nb_all.size())) ||
+                      (e = upload(p, &p->d_nb_off, nb_off.data(), nb_off.size()))))
+        return set_err(MGPU_ERR_NOMEM, "uploading S-matrix descriptors", e);
+    return MGPU_OK;
+}
+
 int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *systems,
                      const mgpu_grid *grids, int njobs, const int *job_sys, const double *job_ered)
 {
@@ -1786,70 +1893,27 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         }
         p->big.push_back(std::move(g));
     }
-    // channel order (CHNSRT, chnsrt.f:16-30: by threshold, equal thresholds keep
-    // their order), open channels and S offsets, for the device S matrix
-    p->nopen.resize(njobs);
-    p->soff.resize(njobs);
-    {
-        bool ok = true;
-        std::vector<int> nb_all, nb_off(nsys);
-        for (int s = 0; s < nsys; ++s) {
-            const mgpu_coupling &c = systems[s];
-            ok = ok && c.n <= smx::kMaxN;
-            nb_off[s] = (int)nb_all.size();
-            std::vector<int> nb(c.n);
-            for (int i = 0; i < c.n; ++i) nb[i] = i;
-            for (int i = 0; i + 1 < c.n; ++i)
-                for (int j = i + 1; j < c.n; ++j) {
-                    const double a = c.eint[nb[i]], bb = c.eint[nb[j]];
-                    if (a <= bb || std::fabs(a - bb) < 1.0e-11) continue;
-                    std::swap(nb[i], nb[j]);
-                }
-            nb_all.insert(nb_all.end(), nb.begin(), nb.end());
-        }
-        std::vector<smx::SJob> sj, sjg;
-        size_t so = 0, scr = 0;
-        for (int j = 0; j < njobs; ++j) {
-            const mgpu_coupling &c = systems[job_sys[j]];
-            int no = 0;
-            for (int i = 0; i < c.n; ++i) no += (job_ered[j] - c.eint[i] > 0.0) ? 1 : 0;
-            p->nopen[j] = no;
-            p->soff[j] = so;
-            so += (size_t)no * no;
-            smx::SJob q;
-            q.sys = job_sys[j];
-            q.nopen = no;
-            q.out = j;
-            q.pad = 0;
-            q.ered = job_ered[j];
-            q.yoff = (long long)p->yoff[j];
-            q.soff = (long long)p->soff[j];
-            q.scr = 0;
-            if (c.n <= smx::kMaxNShared) {
-                p->s_smem = std::max(p->s_smem, smx::smem_bytes(c.n, no));
-                sj.push_back(q);
-            } else {
-                if (no > 0) {
-                    q.scr = (long long)scr;
-                    scr += smx::mat_doubles(c.n, no);
-                }
-                p->s_smem_g = std::max(p->s_smem_g, smx::chan_smem_bytes(c.n));
-                sjg.push_back(q);
-            }
-        }
-        p->selems = so;
-        p->sscr_elems = scr;
-        p->ns_small = (int)sj.size();
-        p->ns_large = (int)sjg.size();
-        p->s_ok = ok;
-        if (ok && njobs > 0 &&
-            ((!sj.empty() && (e = upload(p, &p->d_sjobs, sj.data(), sj.size()))) ||
-             (!sjg.empty() && (e = upload(p, &p->d_sjobs_g, sjg.data(), sjg.size()))) ||
-             (e = upload(p, &p->d_nb, nb_all.data(), nb_all.size())) ||
-             (e = upload(p, &p->d_nb_off, nb_off.data(), nb_off.size())))) {
-            delete p;
-            return set_err(MGPU_ERR_NOMEM, "uploading S-matrix descriptors", e);
-        }
+    // inputs of Y -> S: the couplings' EINT and CENT, the grids' last radius
+    p->s_ok = true;
+    p->s_eint.resize(nsys);
+    p->s_deint.resize(nsys);
+    p->s_dcent.resize(nsys);
+    p->s_devec.assign(nsys, nullptr);
+    p->s_rmatch.resize(nsys);
+    for (int s = 0; s < nsys; ++s) {
+        p->s_ok = p->s_ok && systems[s].n <= smx::kMaxN;
+        p->s_eint[s].assign(systems[s].eint, systems[s].eint + systems[s].n);
+        p->s_deint[s] = hs[s].eint;
+        p->s_dcent[s] = hs[s].cent;
+        p->s_rmatch[s] = grids[s].rtab[2 * (size_t)grids[s].nstep];
+        p->sn_max = std::max(p->sn_max, systems[s].n);
+    }
+    p->job_sys.assign(job_sys, job_sys + njobs);
+    p->job_ered.assign(job_ered, job_ered + njobs);
+    int rc0;
+    if (p->s_ok && (rc0 = build_s(p))) {
+        delete p;
+        return rc0;
     }
     *out = p;
     return MGPU_OK;
@@ -2025,6 +2089,24 @@ int mgpu_plan_smatrix_device(mgpu_plan *p, const double *y_dev, double *sr_dev, 
     if (!y_dev || !sr_dev || !si_dev || !status_dev) return set_err(MGPU_ERR_ARG, "null device buffer");
     cudaError_t e;
     cudaStream_t st = (cudaStream_t)stream;
+    if (p->n_evec > 0) {
+        // YTRANS: Y in the asymptotic basis first, into the plan's own buffer
+        if (!p->d_yt && ((e = cudaMalloc(&p->d_yt, std::max<size_t>(p->yelems, 1) * sizeof(double))) ||
+                         (e = cudaMalloc(&p->d_yz, std::max<size_t>(p->yelems, 1) * sizeof(double)))))
+            return set_err(MGPU_ERR_NOMEM, "asymptotic-basis transform buffers", e);
+        const int tx = (p->sn_max + smx::kTT - 1) / smx::kTT;
+        for (int pass = 1; pass <= 2; ++pass)
+            for (int list = 0; list < 2; ++list) {
+                const int cnt = list ? p->ns_large : p->ns_small;
+                const smx::SJob *jl = list ? p->d_sjobs_g : p->d_sjobs;
+                for (int j0 = 0; j0 < cnt; j0 += 65535) {
+                    smx::ytrans_kernel<<<dim3(tx * tx, std::min(65535, cnt - j0)), 256, 0, st>>>(
+                        p->d_sys, jl + j0, pass, y_dev, p->d_yz, p->d_yt);
+                    if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the YTRANS kernel", e);
+                }
+            }
+        y_dev = p->d_yt;
+    }
     for (int j0 = 0; j0 < p->ns_small; j0 += 65535) {
         if ((e = set_smem(smx::smatrix_kernel, p->s_smem))) return set_err(MGPU_ERR_CUDA, "S-matrix kernel set-up", e);
         smx::smatrix_kernel<<<std::min(65535, p->ns_small - j0), smx::kThreads, p->s_smem, st>>>(
@@ -2042,6 +2124,77 @@ int mgpu_plan_smatrix_device(mgpu_plan *p, const double *y_dev, double *sr_dev, 
             if ((e = cudaGetLastError())) return set_err(MGPU_ERR_CUDA, "launching the S-matrix kernel", e);
         }
     }
+    return MGPU_OK;
+}
+
+int mgpu_plan_set_asymptote(mgpu_plan *p, int sys, const double *eint, const double *cent, const double *evec,
+                            double rmatch)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (sys < 0 || sys >= p->nsys) return set_err(MGPU_ERR_ARG, "system index out of range");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 1024 in every system");
+    if (!eint || !cent) return set_err(MGPU_ERR_ARG, "EINT/CENT null");
+    const int n = p->sys_n[sys];
+    for (int i = 0; i < n; ++i)
+        if (!std::isfinite(eint[i]) || !(cent[i] > -1.0e-10)) return set_err(MGPU_ERR_ARG, "bad EINT or CENT");
+    if (!(rmatch > 0.0) || !std::isfinite(rmatch)) return set_err(MGPU_ERR_ARG, "RMATCH must be positive");
+    cudaError_t e;
+    double *de = nullptr, *dc = nullptr, *dv = nullptr;
+    if ((e = upload(p, &de, eint, n)) || (e = upload(p, &dc, cent, n)) ||
+        (evec && (e = upload(p, &dv, evec, (size_t)n * n))))
+        return set_err(MGPU_ERR_NOMEM, "uploading an asymptotic basis", e);
+    // the previous setting's arrays, unless they are the coupling's own
+    if (p->s_devec[sys]) {
+        p->dfree(const_cast<double *>(p->s_deint[sys]));
+        p->dfree(const_cast<double *>(p->s_dcent[sys]));
+        p->dfree(const_cast<double *>(p->s_devec[sys]));
+        --p->n_evec;
+    }
+    p->s_eint[sys].assign(eint, eint + n);
+    p->s_deint[sys] = de;
+    p->s_dcent[sys] = dc;
+    p->s_devec[sys] = dv;
+    p->s_rmatch[sys] = rmatch;
+    if (dv) ++p->n_evec;
+    return build_s(p);
+}
+
+int mgpu_plan_smatrix_host(mgpu_plan *p, const double *y, double *sr, double *si, int *status)
+{
+    if (!p) return set_err(MGPU_ERR_ARG, "null plan");
+    if (!p->s_ok) return set_err(MGPU_ERR_UNSUPPORTED, "device S matrices need N <= 1024 in every system");
+    if (p->njobs == 0) return MGPU_OK;
+    if (!y || !status || (p->selems && (!sr || !si))) return set_err(MGPU_ERR_ARG, "null host buffer");
+    cudaError_t e;
+    if (!p->own && (e = cudaStreamCreateWithFlags(&p->own, cudaStreamNonBlocking)))
+        return set_err(MGPU_ERR_CUDA, "plan stream", e);
+    if (p->y_cap < p->yelems) {
+        if (p->d_y) cudaFree(p->d_y);
+        p->d_y = nullptr;
+        if ((e = cudaMalloc(&p->d_y, p->yelems * sizeof(double)))) return set_err(MGPU_ERR_NOMEM, "Y buffer", e);
+        p->y_cap = p->yelems;
+    }
+    if (!p->d_status && (e = cudaMalloc(&p->d_status, (size_t)p->njobs * sizeof(int))))
+        return set_err(MGPU_ERR_NOMEM, "status buffer", e);
+    if (p->selems && p->s_cap < p->selems) {
+        if (p->d_sr) cudaFree(p->d_sr);
+        if (p->d_si) cudaFree(p->d_si);
+        p->d_sr = p->d_si = nullptr;
+        if ((e = cudaMalloc(&p->d_sr, p->selems * sizeof(double))) ||
+            (e = cudaMalloc(&p->d_si, p->selems * sizeof(double))))
+            return set_err(MGPU_ERR_NOMEM, "S buffers", e);
+        p->s_cap = p->selems;
+    }
+    if ((e = cudaMemcpyAsync(p->d_y, y, p->yelems * sizeof(double), cudaMemcpyHostToDevice, p->own)) ||
+        (e = cudaMemcpyAsync(p->d_status, status, (size_t)p->njobs * sizeof(int), cudaMemcpyHostToDevice, p->own)))
+        return set_err(MGPU_ERR_CUDA, "copying Y in", e);
+    int rc = mgpu_plan_smatrix_device(p, p->d_y, p->d_sr, p->d_si, p->d_status, p->own);
+    if (rc) return rc;
+    if ((p->selems && ((e = cudaMemcpyAsync(sr, p->d_sr, p->selems * sizeof(double), cudaMemcpyDeviceToHost, p->own)) ||
+                       (e = cudaMemcpyAsync(si, p->d_si, p->selems * sizeof(double), cudaMemcpyDeviceToHost, p->own)))) ||
+        (e = cudaMemcpyAsync(status, p->d_status, (size_t)p->njobs * sizeof(int), cudaMemcpyDeviceToHost, p->own)) ||
+        (e = cudaStreamSynchronize(p->own)))
+        return set_err(MGPU_ERR_CUDA, "copying S out", e);
     return MGPU_OK;
 }
 

@@ -277,6 +277,38 @@ class Plan:
             raise PropagatorError(f"run (S): {_lib.status_string(rc)}: {_lib.last_error()}", rc)
         return sr, si, nodes, status, kfail
 
+    def set_asymptote(self, sys: int, eint, cent, evec=None, rmatch: float | None = None):
+        """YTRANS's output for system ``sys`` (molscat_b200.ytrans): the
+        asymptotic channels' thresholds EINT and L(L+1) values CENT, the basis
+        EVEC (columns; None if Y is already in it) and the matching radius
+        (default: the segment's last radius).  Y -> S then transforms Y to
+        that basis and matches there; NOPEN and the S layout follow."""
+        L = _lib.load()
+        n = self.systems[sys].n
+        e = np.ascontiguousarray(eint, dtype=np.float64).reshape(n)
+        c = np.ascontiguousarray(cent, dtype=np.float64).reshape(n)
+        v = None if evec is None else np.asfortranarray(np.asarray(evec, dtype=np.float64).reshape(n, n))
+        r = float(self.segments[sys].rtab[-1]) if rmatch is None else float(rmatch)
+        rc = L.mgpu_plan_set_asymptote(self._handle, int(sys), e.ctypes.data_as(_dp), c.ctypes.data_as(_dp),
+                                       None if v is None else v.ravel(order="F").ctypes.data_as(_dp), r)
+        if rc != 0:
+            raise PropagatorError(f"asymptote: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+
+    def smatrix_host(self, ybuf: np.ndarray, status=None):
+        """Y -> K -> S on the device from host matrices at the matching radius
+        (the plan's Y layout).  Returns (SR buffer, SI buffer, status)."""
+        L = _lib.load()
+        ns = int(L.mgpu_plan_s_elems(self._handle))
+        y = np.ascontiguousarray(ybuf, dtype=np.float64)
+        sr = np.zeros(max(ns, 1))
+        si = np.zeros(max(ns, 1))
+        st = np.zeros(self.njobs, dtype=np.int32) if status is None else np.array(status, dtype=np.int32)
+        rc = L.mgpu_plan_smatrix_host(self._handle, y.ctypes.data_as(_dp), sr.ctypes.data_as(_dp),
+                                      si.ctypes.data_as(_dp), st.ctypes.data_as(_ip))
+        if rc != 0:
+            raise PropagatorError(f"S: {_lib.status_string(rc)}: {_lib.last_error()}", rc)
+        return sr, si, st
+
     def unpack_s(self, buf: np.ndarray, j: int) -> np.ndarray:
         no = self.nopen(j)
         off = int(_lib.load().mgpu_plan_s_offset(self._handle, int(j)))
