@@ -56,6 +56,15 @@ extern "C" {
 /* propagator ids (IPROP values of scctrl.f:170-196) */
 #define MGPU_PROP_LDJ 5  /* Johnson log-derivative, LDPROP */
 #define MGPU_PROP_LDMD 6 /* Manolopoulos diabatic modified log-derivative, MDPROP */
+/* MGPROP (mgprop.f:1-134): the symplectic log-derivative propagator of
+ * Manolopoulos and Gray, the reference's IPROP = 8 with IMGSEL = 4 (CS4,
+ * five stages, four inversions a sector) or 5 (MA5, six stages and
+ * inversions).  Plans only, N <= 40 (the one-warp kernels).  Its grid's
+ * NSTEP is the number of sectors of width DR, and RTAB/PTAB list the radii
+ * where the stages evaluate W, in order (mgpu_ldmg_radii): 4*NSTEP + 1 rows
+ * for CS4, 6*NSTEP for MA5. */
+#define MGPU_PROP_LDMG4 84
+#define MGPU_PROP_LDMG5 85
 
 /* One coupled-channel system: a (JTOT, symmetry block[, field]) basis.
  * Mirrors the arguments and hidden inputs SUMLAM/HAMMAT read
@@ -358,6 +367,11 @@ int mgpu_set_family_for_n(int iprop, int n_lo, int n_hi, int family);
 const char *mgpu_status_string(int status);
 const char *mgpu_last_error(void);   /* text of the last CUDA/argument error */
 int mgpu_max_n(void);                /* largest N the propagators accept (1024) */
+/* The radii MGPROP visits for IPROP = MGPU_PROP_LDMG4 / LDMG5 from RSTART in
+ * NSTEP sectors of DR: sector s starts at RSTART + s*DR and stage k moves R
+ * by a_k*DR (mgprop.f:75-134).  Writes them to rtab (if not NULL) and
+ * returns how many there are (-1 for another IPROP or NSTEP < 1). */
+int mgpu_ldmg_radii(int iprop, double rstart, double dr, int nstep, double *rtab);
 
 #ifdef __cplusplus
 }

@@ -23,6 +23,8 @@ MGPU_ERR_DEADLINE = 9
 
 MGPU_PROP_LDJ = 5
 MGPU_PROP_LDMD = 6
+MGPU_PROP_LDMG4 = 84  # MGPROP, IMGSEL = 4 (CS4)
+MGPU_PROP_LDMG5 = 85  # MGPROP, IMGSEL = 5 (MA5)
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -53,7 +55,7 @@ EXPORTS = (
     "mgpu_plan_s_elems", "mgpu_plan_s_offset", "mgpu_plan_nopen", "mgpu_plan_smatrix_device",
     "mgpu_plan_run_host_smatrix", "mgpu_plan_set_asymptote", "mgpu_plan_smatrix_host",
     "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
-    "mgpu_plan_cancel", "mgpu_plan_set_time_limit", "mgpu_set_step_wait_limit",
+    "mgpu_plan_cancel", "mgpu_plan_set_time_limit", "mgpu_set_step_wait_limit", "mgpu_ldmg_radii",
 )
 
 _lib = None
@@ -115,6 +117,7 @@ def load(path: str | None = None):
     L.mgpu_plan_run_host_smatrix.argtypes = [vp, _dp, _dp, _dp, _ip, _ip, _ip]
     L.mgpu_plan_set_asymptote.argtypes = [vp, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double]
     L.mgpu_plan_smatrix_host.argtypes = [vp, _dp, _dp, _dp, _ip]
+    L.mgpu_ldmg_radii.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp]
     ll = ctypes.c_longlong
     L.mgpu_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_size_t, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int]

@@ -574,5 +574,120 @@ ldj_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restric
     }
 }
 
+// ---------------------------------------------------------------------------
+// MGPROP step loop (the symplectic log-derivative propagator of Manolopoulos
+// and Gray, mgprop.f:63-134), one warp per job.  Per sector, stage k forms
+// X = Y + b_k h W(R) and, where a_k != 0, Y = [I - (I + a_k h X)^-1]/(a_k h)
+// (the negative pivots of I + a_k h X added to NODES, subtracted where
+// a_k < 0); R advances by a_k h.  W of stage k of sector s is row
+// s*stride + k of the radial tables (stride = stages, or stages - 1 when
+// a_M = 0 and the last stage's W serves as the next sector's first).
+// ---------------------------------------------------------------------------
+struct MGCoef {
+    int m, stride;
+    double a[6], b[6];
+};
+// Table I of D. E. Manolopoulos and S. K. Gray, J. Chem. Phys. 102, 9214
+// (1995): [0] CS4 (IMGSEL = 4), [1] McLachlan and Atela's MA5 (IMGSEL = 5).
+// The host lays out the radial tables from the same numbers.
+#define MGPU_MG_COEFS { \
+        {5, 4, \
+         {0.20517766154229, 0.40302128160421, -0.12092087633891, 0.51272193319241, 0.0, 0.0}, \
+         {0.061758858135626, 0.33897802655364, 0.61479130717558, -0.14054801465937, 0.12501982279453, 0.0}}, \
+        {6, 6, \
+         {0.33983962583911, -0.088601336903027, 0.58585647682596, -0.60303935653649, 0.32358079655470, \
+          0.44236379421975}, \
+         {0.11939002928757, 0.69892737038248, -0.17131235827160, 0.40126950225135, 0.010705081848236, \
+          -0.058979625498031}}, \
+    }
+constexpr MGCoef kMGCoef[2] = MGPU_MG_COEFS;
+// the device copy, initialised from the same literal list
+__constant__ MGCoef c_mg[2] = MGPU_MG_COEFS;
+#undef MGPU_MG_COEFS
+
+template <int NT>
+__global__ void __launch_bounds__(32 * kWPB)
+ldmg_prop_frag_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int njobs, int method,
+                      double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                      int *__restrict__ kfail_out)
+{
+    constexpr int NTL = G<NT>::NTL;
+    __shared__ __align__(16) double pans[kWPB][G<NT>::WSM];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int jix = blockIdx.x * kWPB + warp;
+    if (jix >= njobs) return;
+    const JobDev job = jobs[jix];
+    const SysDev &S = systems[job.sys];
+    const MGCoef &C = c_mg[method];
+    double *pan = pans[warp];
+    const int n = S.n;
+    const double ered = job.ered;
+    const double h = S.dr;
+    double *yj = y + job.yoff;
+    const int r = lane >> 2, q = lane & 3;
+
+    double a[NTL][2], w[NTL][2];
+    load_lower_frag<NT>(yj, n, lane, a);
+    int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
+    for (int sec = 0; sec < S.nstep; ++sec) {
+        if (stop_poll_step(sec + 1)) {
+            int stop = lane == 0 ? stop_requested(S.ctl, t0) : MGPU_OK;
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = sec + 1;
+                break;
+            }
+        }
+#pragma unroll 1
+        for (int k = 0; k < C.m; ++k) {
+            w_frag<NT>(S, lane, sec * C.stride + k, ered, true, w);
+            const double bh = C.b[k] * h;
+#pragma unroll
+            for (int t = 0; t < NTL; ++t)
+#pragma unroll
+                for (int s = 0; s < 2; ++s) a[t][s] = fma(bh, w[t][s], a[t][s]);  // X = Y + b_k h W
+            const double ak = C.a[k];
+            if (ak == 0.0) continue;  // Y = X
+            const double ah = ak * h;
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int J = 0; J <= I; ++J)
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                        a[tix(I, J)][s] = ah * a[tix(I, J)][s] + (dg ? 1.0 : 0.0);  // I + a_k h X
+                    }
+            int bad = SWEEP_OK;
+            const int cnt = warp_sweep_invert<NT>(a, pan, n, lane, bad);  // a = -(I + a_k h X)^-1
+            if (bad != SWEEP_OK) {
+                status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+                kfail = sec + 1;
+                break;
+            }
+            nodes += ak >= 0.0 ? cnt : -cnt;
+            const double d1 = 1.0 / ah;
+#pragma unroll
+            for (int I = 0; I < NT; ++I)
+#pragma unroll
+                for (int J = 0; J <= I; ++J)
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const bool dg = (I == J) && (r == 2 * q + s) && (8 * I + r < n);
+                        a[tix(I, J)][s] = (a[tix(I, J)][s] + (dg ? 1.0 : 0.0)) * d1;  // [I - inverse]/(a_k h)
+                    }
+        }
+        if (status != MGPU_OK) break;
+    }
+    if (status == MGPU_OK) store_full_frag<NT>(yj, n, lane, 1.0, a);
+    if (lane == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes : 0;
+    }
+}
+
 }  // namespace wf
 }  // namespace mgpu

@@ -672,8 +672,12 @@ static size_t tile_elems(int b) { return (size_t)bucket_edge(b) * bucket_edge(b)
 static size_t matrix_elems(int b) { return tile_elems(b) * ntiles_of(b); }         // doubles per tiled matrix
 
 // LDJ keeps two tiled matrices in shared memory: CTA buckets up to N = 128.
+static bool is_ldmg(int iprop) { return iprop == MGPU_PROP_LDMG4 || iprop == MGPU_PROP_LDMG5; }
+
+// LDMG runs on the one-warp kernels only (N <= 40).
 static bool bucket_allows(int b, int iprop)
 {
+    if (is_ldmg(iprop)) return kBuckets[b].kind == KIND_FRAG8;
     return !(iprop == MGPU_PROP_LDJ && kBuckets[b].kind == KIND_CTA8 && kBuckets[b].nt > 16);
 }
 
@@ -700,7 +704,7 @@ static int bucket_of_kind(int n, int iprop, int kind)
 
 static int bucket_for(int n, int iprop = MGPU_PROP_LDMD, bool tuned = true)
 {
-    if (tuned) {
+    if (tuned && !is_ldmg(iprop)) {
         std::lock_guard<std::mutex> lk(g_family_mu);
         for (const auto &r : g_family_ranges)
             if ((r.iprop == 0 || r.iprop == iprop) && n >= r.lo && n <= r.hi && r.family != 0) {
@@ -860,6 +864,9 @@ static cudaError_t launch_prop(int iprop, int b, int njobs, size_t smem, int vl_
             if ((e = set_smem(wf::ldmd_prop_frag_kernel<t>, smem))) return e;                                 \
             wf::ldmd_prop_frag_kernel<t><<<blocks, 32 * wf::kWPB, smem, st>>>(sys, jobs, njobs, y, nodes,     \
                                                                               status, kfail);                 \
+        } else if (is_ldmg(iprop)) {                                                                          \
+            wf::ldmg_prop_frag_kernel<t><<<blocks, 32 * wf::kWPB, 0, st>>>(                                   \
+                sys, jobs, njobs, iprop == MGPU_PROP_LDMG5 ? 1 : 0, y, nodes, status, kfail);                 \
         } else {                                                                                              \
             wf::ldj_prop_frag_kernel<t><<<blocks, 32 * wf::kWPB, 0, st>>>(sys, jobs, njobs, y, nodes, status, \
                                                                           kfail);                             \
@@ -1201,7 +1208,9 @@ static int build_sysdev(const mgpu_coupling &c, const mgpu_grid &g, int iprop, i
     d.kind = frag_layout(b) ? 1 : 0;
     d.conlen = c.conlen;
     d.dr = g.dr;
-    const size_t nr = 2 * (size_t)g.nstep + 1;
+    // rows of the radial tables: MDPROP/LDPROP's half steps, MGPROP's stages
+    const size_t nr = is_ldmg(iprop) ? (size_t)(iprop == MGPU_PROP_LDMG5 ? 6 * (size_t)g.nstep : 4 * (size_t)g.nstep + 1)
+                                     : 2 * (size_t)g.nstep + 1;
     double *dv = nullptr, *de = nullptr, *dc = nullptr, *drt = nullptr, *dpt = nullptr, *dq = nullptr;
     int *di = nullptr;
     std::vector<double> pt(std::max<size_t>(nr * c.nham, 1), 0.0);
@@ -1434,6 +1443,25 @@ static int check_coupling(const mgpu_coupling *c, const mgpu_grid *g, int iprop)
 }
 
 extern "C" {
+
+int mgpu_ldmg_radii(int iprop, double rstart, double dr, int nstep, double *rtab)
+{
+    if (!is_ldmg(iprop) || nstep < 1) return -1;
+    const wf::MGCoef &m = wf::kMGCoef[iprop == MGPU_PROP_LDMG5 ? 1 : 0];
+    int cnt = 0;
+    for (int s = 0; s < nstep; ++s) {
+        double r = rstart + s * dr;  // mgprop.f:76
+        for (int k = 0; k < m.m; ++k) {
+            const bool reused = (k == 0 && s > 0 && m.stride < m.m);  // the previous sector's last W
+            if (!reused) {
+                if (rtab) rtab[cnt] = r;
+                ++cnt;
+            }
+            r = r + m.a[k] * dr;  // mgprop.f:129
+        }
+    }
+    return cnt;
+}
 
 int mgpu_max_n(void)
 {
@@ -1680,10 +1708,13 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
 {
     if (!out) return set_err(MGPU_ERR_ARG, "null plan pointer");
     *out = nullptr;
-    if (iprop != MGPU_PROP_LDMD && iprop != MGPU_PROP_LDJ) return set_err(MGPU_ERR_ARG, "IPROP must be 5 or 6");
+    if (iprop != MGPU_PROP_LDMD && iprop != MGPU_PROP_LDJ && !is_ldmg(iprop))
+        return set_err(MGPU_ERR_ARG, "IPROP must be 5, 6, 84 or 85");
     if (nsys < 1 || njobs < 0 || !systems || !grids || (njobs > 0 && (!job_sys || !job_ered)))
         return set_err(MGPU_ERR_ARG, "bad system/job arrays");
     for (int s = 0; s < nsys; ++s) {
+        if (is_ldmg(iprop) && systems[s].n > 40)
+            return set_err(MGPU_ERR_UNSUPPORTED, "LDMG runs on the one-warp kernels: N <= 40");
         int rc = check_coupling(&systems[s], &grids[s], iprop);
         if (rc) return rc;
     }
@@ -1799,8 +1830,18 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         off += (size_t)n * (size_t)n;
         const double nh = systems[job_sys[j]].nham;
         const double ns = grids[job_sys[j]].nstep;
-        p->flops += (3.0 * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
-        p->flops_prop += ((iprop == MGPU_PROP_LDMD ? 2.0 : 3.0) * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
+        if (is_ldmg(iprop)) {
+            // per sector: an inversion for every stage with a_k != 0, a W for every stage
+            const wf::MGCoef &m = wf::kMGCoef[iprop == MGPU_PROP_LDMG5 ? 1 : 0];
+            int ninv = 0;
+            for (int k = 0; k < m.m; ++k) ninv += m.a[k] != 0.0 ? 1 : 0;
+            const double f = (ninv * n * n * n + m.m * nh * n * (n + 1.0)) * ns;
+            p->flops += f;
+            p->flops_prop += f;
+        } else {
+            p->flops += (3.0 * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
+            p->flops_prop += ((iprop == MGPU_PROP_LDMD ? 2.0 : 3.0) * n * n * n + 2.0 * nh * n * (n + 1.0)) * ns;
+        }
     }
     p->yelems = off;
     std::vector<int> order(njobs);
@@ -1905,7 +1946,8 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
         p->s_eint[s].assign(systems[s].eint, systems[s].eint + systems[s].n);
         p->s_deint[s] = hs[s].eint;
         p->s_dcent[s] = hs[s].cent;
-        p->s_rmatch[s] = grids[s].rtab[2 * (size_t)grids[s].nstep];
+        p->s_rmatch[s] = is_ldmg(iprop) ? grids[s].rtab[0] + grids[s].nstep * grids[s].dr
+                                        : grids[s].rtab[2 * (size_t)grids[s].nstep];
         p->sn_max = std::max(p->sn_max, systems[s].n);
     }
     p->job_sys.assign(job_sys, job_sys + njobs);

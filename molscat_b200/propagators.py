@@ -22,7 +22,10 @@ from typing import Callable, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import Coupling_C, Grid_C, MGPU_PROP_LDJ, MGPU_PROP_LDMD
+from ._lib import Coupling_C, Grid_C, MGPU_PROP_LDJ, MGPU_PROP_LDMD, MGPU_PROP_LDMG4, MGPU_PROP_LDMG5
+
+# plan propagators: MDPROP, LDPROP and MGPROP with IMGSEL = 4 / 5
+PROPS = {"LDMD": MGPU_PROP_LDMD, "LDJ": MGPU_PROP_LDJ, "LDMG4": MGPU_PROP_LDMG4, "LDMG5": MGPU_PROP_LDMG5}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -89,28 +92,54 @@ def radial_grid(rstart: float, dr: float, nstep: int) -> np.ndarray:
     return r
 
 
+def ldmg_radii(prop: str, rstart: float, dr: float, nstep: int) -> np.ndarray:
+    """The radii MGPROP's stages visit ("LDMG4": CS4, 4*NSTEP + 1 of them;
+    "LDMG5": MA5, 6*NSTEP), from the library's own coefficients."""
+    L = _lib.load()
+    ip = PROPS[prop]
+    cnt = int(L.mgpu_ldmg_radii(ip, float(rstart), float(dr), int(nstep), None))
+    if cnt < 0:
+        raise ValueError(f"{prop}: not an LDMG propagator, or NSTEP < 1")
+    out = np.empty(cnt)
+    L.mgpu_ldmg_radii(ip, float(rstart), float(dr), int(nstep), out.ctypes.data_as(_dp))
+    return out
+
+
 @dataclass
 class Segment:
-    """One propagation segment: NSTEP, DR and the P table at every radius."""
+    """One propagation segment: NSTEP, DR and the P table at every radius
+    (kind "LD": MDPROP/LDPROP's 2*NSTEP+1 half-step radii; "LDMG4"/"LDMG5":
+    the MGPROP stages' radii, ldmg_radii)."""
     nstep: int
     dr: float
     rtab: np.ndarray
     ptab: np.ndarray
+    kind: str = "LD"
 
     @classmethod
     def build(cls, rstart: float, dr: float, nstep: int, potential: Callable[[float], np.ndarray],
-              nham: int) -> "Segment":
-        rtab = radial_grid(rstart, dr, nstep)
+              nham: int, kind: str = "LD") -> "Segment":
+        rtab = radial_grid(rstart, dr, nstep) if kind == "LD" else ldmg_radii(kind, rstart, dr, nstep)
         ptab = np.empty((rtab.size, max(nham, 1)))
         for k, r in enumerate(rtab):
             ptab[k, :nham] = potential(float(r))[:nham]
-        return cls(nstep, dr, rtab, ptab)
+        return cls(nstep, dr, rtab, ptab, kind)
+
+    def rows(self) -> int:
+        if self.kind == "LD":
+            return 2 * self.nstep + 1
+        if self.kind == "LDMG4":
+            return 4 * self.nstep + 1
+        if self.kind == "LDMG5":
+            return 6 * self.nstep
+        raise ValueError(f"segment kind {self.kind!r}")
 
     def __post_init__(self):
         self.rtab = np.ascontiguousarray(self.rtab, dtype=np.float64)
         self.ptab = np.ascontiguousarray(self.ptab, dtype=np.float64)
-        if self.rtab.shape[0] != 2 * self.nstep + 1 or self.ptab.shape[0] != 2 * self.nstep + 1:
-            raise ValueError("tables need 2*NSTEP+1 rows")
+        nr = self.rows()
+        if self.rtab.shape[0] != nr or self.ptab.shape[0] != nr:
+            raise ValueError(f"tables need {nr} rows for a {self.kind} segment of NSTEP = {self.nstep}")
 
     def c_struct(self) -> Grid_C:
         return Grid_C(int(self.nstep), float(self.dr), self.rtab.ctypes.data_as(_dp),
@@ -216,9 +245,13 @@ class Plan:
 
     def __post_init__(self):
         L = _lib.load()
-        self.iprop = MGPU_PROP_LDMD if self.prop == "LDMD" else MGPU_PROP_LDJ
-        if self.prop not in ("LDMD", "LDJ"):
+        if self.prop not in PROPS:
             raise ValueError(self.prop)
+        self.iprop = PROPS[self.prop]
+        want = self.prop if self.prop.startswith("LDMG") else "LD"
+        for g in self.segments:
+            if g.kind != want:
+                raise ValueError(f"a {self.prop} plan needs {want} segments, got {g.kind}")
         self.job_sys = np.ascontiguousarray(self.job_sys, dtype=np.int32)
         self.job_ered = np.ascontiguousarray(self.job_ered, dtype=np.float64)
         ns = len(self.systems)

@@ -163,6 +163,50 @@ def ldprop(c: Coupling, rtab, ptab, nstep, dr, ered, y0):
     return _propagate("oracle_ldprop", c, rtab, ptab, nstep, dr, ered, y0)
 
 
+# Symplectic integrator coefficients a_k (R advances by a_k h) and b_k (the
+# W kick), Table I of D. E. Manolopoulos and S. K. Gray, J. Chem. Phys. 102,
+# 9214 (1995): CS4 (five stages, a_5 = 0) and McLachlan-Atela's MA5 (six).
+MG_COEFFS = {
+    4: ((0.20517766154229, 0.40302128160421, -0.12092087633891, 0.51272193319241, 0.0),
+        (0.061758858135626, 0.33897802655364, 0.61479130717558, -0.14054801465937, 0.12501982279453)),
+    5: ((0.33983962583911, -0.088601336903027, 0.58585647682596, -0.60303935653649, 0.32358079655470,
+         0.44236379421975),
+        (0.11939002928757, 0.69892737038248, -0.17131235827160, 0.40126950225135, 0.010705081848236,
+         -0.058979625498031)),
+}
+
+
+def mgprop(c: Coupling, sysm, rstart: float, dr: float, nstep: int, ered: float, y0, imgsel: int = 4):
+    """MGPROP (mgprop.f:63-134) restated: per sector, stage k forms
+    X = Y + b_k h W(R) and, where a_k != 0, Y = [I - (I + a_k h X)^-1]/(a_k h),
+    adding the negative pivots of I + a_k h X to NODES (subtracting them for
+    a_k < 0); R advances by a_k h.  Returns (Y, NODES)."""
+    a, b = MG_COEFFS[imgsel]
+    m = len(a)
+    n = c.n
+    y = np.array(y0, dtype=np.float64)
+    nodes = 0
+    eye = np.eye(n)
+    w = None
+    for s in range(nstep):
+        r = rstart + s * dr
+        for k in range(m):
+            # with a_M = 0 the last stage's W (at the accumulated end of the
+            # previous sector) serves as this sector's first (mgprop.f:82-93)
+            if not (k == 0 and s > 0 and a[m - 1] == 0.0):
+                w = hammat(c, r, sysm.pvec(r), ered)
+            x = y + (b[k] * dr) * w
+            if a[k] != 0.0:
+                inv, cnt = syminv((a[k] * dr) * x + eye)
+                inv = np.tril(inv) + np.tril(inv, -1).T
+                nodes += cnt if a[k] >= 0.0 else -cnt
+                y = (eye - inv) * (1.0 / (a[k] * dr))
+            else:
+                y = x
+            r = r + a[k] * dr
+    return 0.5 * (y + y.T), nodes
+
+
 def radial_grid(rstart: float, dr: float, nstep: int) -> np.ndarray:
     """Radii in the order MDPROP/LDPROP visit them: R=RSTART, then R=R+H
     repeated (mdprop.f:69,117,203; ldprop.f:30,57,105)."""
@@ -575,7 +619,9 @@ class ScatteringResult:
 def molscat_smatrix(sysm: Itype1, jtot: int, block: int, energies, rmin: float, rmax: float,
                     steps: float, propagator: str = "LDMD", irmset: int = 9,
                     iscru: bool = True):
-    """One (JTOT, block) of a MOLSCAT run with a single LDMD or LDJ segment.
+    """One (JTOT, block) of a MOLSCAT run with a single LDMD, LDJ or LDMG
+    segment ("LDMG4" / "LDMG5": MGPROP with IMGSEL = 4 or 5, the same step
+    count as the log-derivative propagators).
 
     Follows mol.driver.f:1141-1146,1453,1488-1549 (EREDMX = highest energy when
     ISCRU is set, FINDRM at EREDMX, CAYS = CALCK(0, EREDMX)) and scctrl.f
@@ -600,6 +646,10 @@ def molscat_smatrix(sysm: Itype1, jtot: int, block: int, energies, rmin: float, 
             y, nodes, st, kf = mdprop(c, rtab, ptab, nstep, dr, ered, y0)
         elif propagator == "LDJ":
             y, nodes, st, kf = ldprop(c, rtab, ptab, nstep, dr, ered, y0)
+        elif propagator in ("LDMG4", "LDMG5"):
+            y, nodes = mgprop(c, sysm, rstart, dr, nstep, ered, y0, int(propagator[-1]))
+            st, kf = 0, 0
+            rtab = np.array([rstart, rstart + nstep * dr])
         else:
             raise ValueError(propagator)
         if st != 0:

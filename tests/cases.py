@@ -22,7 +22,7 @@ def rotor_case(jtot, block, nstep=4000, energies_cm=(150.0,), rmin_a=2.5, rmax_a
     return c, seg, jobs
 
 
-def random_case(n, nstep, seed, nham_pot=3, ivlfl=0, nconst=0, nrsq=0, conlen=0.0, inward=False):
+def random_case(n, nstep, seed, nham_pot=3, ivlfl=0, nconst=0, nrsq=0, conlen=0.0, inward=False, kind="LD"):
     """A random but physical-looking coupled-channel problem: a Lennard-Jones
     isotropic term plus anisotropic exponential/power terms with random
     symmetric coupling coefficients, random thresholds and L values.
@@ -31,7 +31,9 @@ def random_case(n, nstep, seed, nham_pot=3, ivlfl=0, nconst=0, nrsq=0, conlen=0.
     not added, hammat.f:95).  nrsq: L(L+1) enters through a VL term with
     P = min(1/R^2, 1e16) (hammat.f:77-83,89).  ivlfl: VL slots read P through
     a random permutation IV, and NVLBLK = NHAM+1 leaves a slot SUMLAM must
-    skip.  inward: propagate from the long-range side in (DR < 0)."""
+    skip.  inward: propagate from the long-range side in (DR < 0).  kind: the
+    segment's radii ("LD", or "LDMG4"/"LDMG5" for MGPROP's stages); the
+    potential is kept as seg.pvec(R)."""
     rng = np.random.default_rng(seed)
     npair = n * (n + 1) // 2
     eint = np.sort(rng.uniform(0.0, 60.0, n))
@@ -84,11 +86,16 @@ def random_case(n, nstep, seed, nham_pot=3, ivlfl=0, nconst=0, nrsq=0, conlen=0.
 
     r0, r1 = (6.0, 0.85) if inward else (0.85, 6.0)
     dr = (r1 - r0) / nstep
-    rtab = radial_grid(r0, dr, nstep)
+    if kind == "LD":
+        rtab = radial_grid(r0, dr, nstep)
+    else:
+        from molscat_b200.propagators import ldmg_radii
+        rtab = ldmg_radii(kind, r0, dr, nstep)
     ptab = np.stack([pot(float(r)) for r in rtab])
     c = Coupling(n=n, nham=nham, vl=vl, eint=eint, cent=cent, nvlblk=nvlblk, iv=iv if ivlfl else None,
                  ivlfl=ivlfl, nconst=nconst, nrsq=nrsq, conlen=conlen)
-    seg = Segment(nstep, dr, rtab, ptab)
+    seg = Segment(nstep, dr, rtab, ptab, kind)
+    seg.pvec = pot
     ered = float(rng.uniform(20.0, 80.0))
     w0 = _diag_w(c, seg, 0, ered)
     sgn = -1.0 if inward else 1.0

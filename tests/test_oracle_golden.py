@@ -1,7 +1,8 @@
 """Pin the CPU oracle against the reference's own printed S matrices.
 
 examples/output/molscat-all_propagators.output prints the 6x6 open-channel
-S matrix to 14 significant digits for LDMD (IPROPS=6) and LDJ (IPROPS=5),
+S matrix to 14 significant digits for LDMD (IPROPS=6), LDJ (IPROPS=5) and
+the symplectic LDMG (IPROPS=8, IMGSEL=5: MA5),
 ITYPE=1, JTOT=10, block 1, N=12, E=1000 and 900 cm-1 (fixture made by
 tests/golden/make_golden.py).  The restated MOLSCAT driver path (FINDRM,
 DRSET, YINIT, propagator, YTOK, KTOS) must reproduce them within 1e-8.
@@ -20,12 +21,12 @@ def _system(g):
                     terms=[[tuple(t) for t in tl] for tl in s["terms"]], rm=s["rm"], epsil=s["epsil"])
 
 
-@pytest.mark.parametrize("prop", ["LDMD", "LDJ"])
+@pytest.mark.parametrize("prop", ["LDMD", "LDJ", "LDMG"])
 def test_smatrix_matches_reference_output(golden, prop):
     s = golden["system"]
     run = golden["runs"][prop]
     res = O.molscat_smatrix(_system(golden), s["jtot"], s["block"], run["energies_cm"],
-                            s["rmin"], s["rmax"], s["steps"], prop)
+                            s["rmin"], s["rmax"], s["steps"], "LDMG5" if prop == "LDMG" else prop)
     for r, blk, nstep in zip(res, run["smatrix"], run["nstep"]):
         assert r.nstep == nstep
         assert [c + 1 for c in r.nb[: r.nopen]] == [4, 7, 5, 2, 8, 10]
