@@ -59,7 +59,7 @@ extern "C" {
 /* MGPROP (mgprop.f:1-134): the symplectic log-derivative propagator of
  * Manolopoulos and Gray, the reference's IPROP = 8 with IMGSEL = 4 (CS4,
  * five stages, four inversions a sector) or 5 (MA5, six stages and
- * inversions).  Plans only, N <= 40 (the one-warp kernels).  Its grid's
+ * inversions).  Plans only, N <= 200 (the one-warp and one-CTA kernels).  Its grid's
  * NSTEP is the number of sectors of width DR, and RTAB/PTAB list the radii
  * where the stages evaluate W, in order (mgpu_ldmg_radii): 4*NSTEP + 1 rows
  * for CS4, 6*NSTEP for MA5. */

@@ -729,5 +729,103 @@ ldj_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict
     }
 }
 
+// ---------------------------------------------------------------------------
+// MGPROP step loop on one CTA per job (40 < N <= 200): the one-warp
+// kernel's stages (kernels_frag.cuh, ldmg_prop_frag_kernel) with Y as tiles
+// in shared memory and the CTA sweep for the inversions.
+// ---------------------------------------------------------------------------
+template <int NT, int W>
+__global__ void __launch_bounds__(32 * W)
+ldmg_prop_cta_kernel(const SysDev *__restrict__ systems, const JobDev *__restrict__ jobs, int method,
+                     double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+                     int *__restrict__ kfail_out)
+{
+    using C = CG<NT, W>;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ TileRC tab[tabn<NT, W>()];
+    __shared__ int cf[2];
+    __shared__ int s_stop;
+    __shared__ SysDev s_sys;
+    const JobDev job = jobs[blockIdx.x];
+    if (threadIdx.x == 0) s_sys = systems[job.sys];
+    build_table<NT, W>(tab);
+    __syncthreads();
+    const SysDev &S = s_sys;
+    const wf::MGCoef &M = wf::c_mg[method];
+    const int tid = threadIdx.x;
+    double *yt = sm;
+    double *pan = yt + C::TD;
+    double *xs = pan + CSmem<NT, W>::PAN;
+    double *fbuf = xs + CSmem<NT, W>::PAN;
+    const int n = S.n;
+    const double ered = job.ered;
+    const double h = S.dr;
+    double *yj = y + job.yoff;
+    for (int x = tid; x < C::TD; x += C::NTHR) {
+        int i, j;
+        elem_rc(tab, x, i, j);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        yt[x] = (i < n && j < n) ? yj[(size_t)lo * n + hi] : 0.0;
+    }
+    __syncthreads();
+    int nodes = 0, status = MGPU_OK, kfail = 0;
+    const unsigned long long t0 = global_ns();
+    for (int sec = 0; sec < S.nstep && status == MGPU_OK; ++sec) {
+        if (stop_poll_step(sec + 1)) {
+            if (tid == 0) s_stop = stop_requested(S.ctl, t0);
+            __syncthreads();  // the next write comes kStopPoll sectors (and their barriers) later
+            const int stop = s_stop;
+            if (stop != MGPU_OK) {
+                status = stop;
+                kfail = sec + 1;
+                break;
+            }
+        }
+        for (int k = 0; k < M.m; ++k) {
+            const int ir = sec * M.stride + k;
+            const double *P = S.ptab + (size_t)ir * S.nham;
+            const double bh = M.b[k] * h, ak = M.a[k], ah = ak * h;
+            for (int x = tid; x < C::TD; x += C::NTHR) {
+                int i, j;
+                elem_rc(tab, x, i, j);
+                const double xv = fma(bh, w_elem(S, P, x, i, j, ir, ered, true), yt[x]);  // X = Y + b_k h W
+                yt[x] = ak == 0.0 ? xv : ah * xv + ((i == j && i < n) ? 1.0 : 0.0);      // I + a_k h X
+            }
+            __syncthreads();
+            if (ak == 0.0) continue;
+            int bad = SWEEP_OK;
+            const int cnt = cta_invert<NT, W>(yt, pan, xs, fbuf, cf, n, tab, sm + CSmem<NT, W>::extra(1), bad);
+            if (bad != SWEEP_OK) {
+                status = bad == SWEEP_ZERO ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+                kfail = sec + 1;
+                break;
+            }
+            nodes += ak >= 0.0 ? cnt : -cnt;
+            const double d1 = 1.0 / ah;
+            for (int x = tid; x < C::TD; x += C::NTHR) {
+                int i, j;
+                elem_rc(tab, x, i, j);
+                yt[x] = (yt[x] + ((i == j && i < n) ? 1.0 : 0.0)) * d1;  // [I - inverse]/(a_k h)
+            }
+            __syncthreads();
+        }
+    }
+    if (status == MGPU_OK) {
+        for (int x = tid; x < C::TD; x += C::NTHR) {
+            int i, j;
+            elem_rc(tab, x, i, j);
+            if (i < n && j <= i) {
+                yj[(size_t)j * n + i] = yt[x];
+                yj[(size_t)i * n + j] = yt[x];
+            }
+        }
+    }
+    if (tid == 0) {
+        status_out[job.out] = status;
+        kfail_out[job.out] = kfail;
+        nodes_out[job.out] = status == MGPU_OK ? nodes : 0;
+    }
+}
+
 }  // namespace cta
 }  // namespace mgpu

@@ -674,10 +674,10 @@ static size_t matrix_elems(int b) { return tile_elems(b) * ntiles_of(b); }      
 // LDJ keeps two tiled matrices in shared memory: CTA buckets up to N = 128.
 static bool is_ldmg(int iprop) { return iprop == MGPU_PROP_LDMG4 || iprop == MGPU_PROP_LDMG5; }
 
-// LDMG runs on the one-warp kernels only (N <= 40).
+// LDMG runs on the one-warp and one-CTA kernels (N <= 200).
 static bool bucket_allows(int b, int iprop)
 {
-    if (is_ldmg(iprop)) return kBuckets[b].kind == KIND_FRAG8;
+    if (is_ldmg(iprop)) return kBuckets[b].kind == KIND_FRAG8 || kBuckets[b].kind == KIND_CTA8;
     return !(iprop == MGPU_PROP_LDJ && kBuckets[b].kind == KIND_CTA8 && kBuckets[b].nt > 16);
 }
 
@@ -844,6 +844,10 @@ static cudaError_t launch_prop(int iprop, int b, int njobs, size_t smem, int vl_
         if (iprop == MGPU_PROP_LDMD) {                                                                       \
             if ((e = set_smem(cta::ldmd_prop_cta_kernel<t, w>, smem))) return e;                             \
             cta::ldmd_prop_cta_kernel<t, w><<<njobs, 32 * w, smem, st>>>(sys, jobs, y, nodes, status, kfail); \
+        } else if (is_ldmg(iprop)) {                                                                         \
+            if ((e = set_smem(cta::ldmg_prop_cta_kernel<t, w>, smem))) return e;                             \
+            cta::ldmg_prop_cta_kernel<t, w><<<njobs, 32 * w, smem, st>>>(                                    \
+                sys, jobs, iprop == MGPU_PROP_LDMG5 ? 1 : 0, y, nodes, status, kfail);                       \
         } else {                                                                                             \
             if ((e = set_smem(cta::ldj_prop_cta_kernel<t, w>, smem))) return e;                              \
             cta::ldj_prop_cta_kernel<t, w><<<njobs, 32 * w, smem, st>>>(sys, jobs, y, nodes, status, kfail);  \
@@ -1713,8 +1717,8 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     if (nsys < 1 || njobs < 0 || !systems || !grids || (njobs > 0 && (!job_sys || !job_ered)))
         return set_err(MGPU_ERR_ARG, "bad system/job arrays");
     for (int s = 0; s < nsys; ++s) {
-        if (is_ldmg(iprop) && systems[s].n > 40)
-            return set_err(MGPU_ERR_UNSUPPORTED, "LDMG runs on the one-warp kernels: N <= 40");
+        if (is_ldmg(iprop) && systems[s].n > 200)
+            return set_err(MGPU_ERR_UNSUPPORTED, "LDMG runs on the one-warp and one-CTA kernels: N <= 200");
         int rc = check_coupling(&systems[s], &grids[s], iprop);
         if (rc) return rc;
     }

@@ -1,16 +1,17 @@
 """MGPROP, the symplectic log-derivative propagator (mgprop.f; the
 reference's IPROP = 8 with IMGSEL = 4 (CS4) or 5 (MA5)), on the one-warp
-kernels against the oracle's restatement (oracle/oracle.py, mgprop), which
-reproduces the reference's MA5 S matrices of molscat-all_propagators
-(tests/test_oracle_golden.py, 3.5e-12).
+(N <= 40) and one-CTA (N <= 200) kernels against the oracle's restatement
+(oracle/oracle.py, mgprop), which reproduces the reference's MA5 S
+matrices of molscat-all_propagators (tests/test_oracle_golden.py, 3.5e-12).
 
 * CPU: the library's stage radii (mgpu_ldmg_radii) equal an independent
   accumulation R = RSTART + s*DR, R += a_k*DR (mgprop.f:76,129), bit for
-  bit, with CS4's last-stage reuse; the plan rejects N > 40 and a segment of
-  the wrong kind.
+  bit, with CS4's last-stage reuse; a plan rejects a segment of the wrong
+  kind.
 * GPU: the reference's golden S matrices (N = 12, 8072 sectors, both
-  energies) with the GPU propagating; random systems N = 5..40 for CS4 and
-  MA5 against the oracle (Y within 5e-8 of max|Y|, NODES exact).
+  energies) with the GPU propagating; random systems N = 5..150 for CS4 and
+  MA5 against the oracle (Y within 5e-8 of max|Y|, NODES exact); N > 200
+  refused.
 """
 import numpy as np
 import pytest
@@ -70,10 +71,11 @@ class _Pot:
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["LDMG4", "LDMG5"])
-@pytest.mark.parametrize("n", [5, 12, 24, 33, 40])
+@pytest.mark.parametrize("n", [5, 12, 24, 33, 40, 57, 106, 150])
 def test_gpu_random_systems_match_oracle(gpu, kind, n):
+    """N <= 40 on the one-warp kernels, above on the one-CTA kernels."""
     from oracle import oracle as O
-    nstep = 300
+    nstep = 300 if n <= 64 else 80
     c, seg, ered, y0 = cases.random_case(n, nstep, seed=60 + n, kind=kind)
     erg = ered + np.array([0.0, 3.0])
     plan = Plan(kind, [c], [seg], np.zeros(2, dtype=np.int32), erg)
@@ -86,6 +88,14 @@ def test_gpu_random_systems_match_oracle(gpu, kind, n):
         assert nodes[j] == no
         assert np.abs(yg - yo).max() <= 5e-8 * np.abs(yo).max()
     plan.close()
+
+
+@pytest.mark.gpu
+def test_gpu_refuses_n_above_200(gpu):
+    from molscat_b200.propagators import PropagatorError
+    c, seg, ered, y0 = cases.random_case(201, 2, seed=5, kind="LDMG4")
+    with pytest.raises(PropagatorError):
+        Plan("LDMG4", [c], [seg], np.zeros(1, dtype=np.int32), np.array([ered]))
 
 
 @pytest.mark.gpu
