@@ -100,6 +100,11 @@ int mgpu_mdprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
                 double *y, int *nodes, int *kfail);
 int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
                 double *z, int *nodes, int *kfail);
+/* mgpu_mgprop replaces MGPROP (mgprop.f:1-134) with IMGSEL = 4 (CS4) or 5
+ * (MA5): g's tables are the stage radii of mgpu_ldmg_radii; y in and out
+ * as MGPROP's Y.  N <= 200. */
+int mgpu_mgprop(int imgsel, const mgpu_coupling *c, const mgpu_grid *g, double ered,
+                double *y, int *nodes, int *kfail);
 
 /* The same two calls in the Fortran calling convention, every argument by
  * reference and no structures, for an ISO_C_BINDING interface block with
@@ -115,6 +120,11 @@ void mgpu_ldprop_f(const int *n, const int *nham, const int *nvlblk, const int *
                    const int *nrsq, const double *conlen, double *z, const double *vl, const int *iv,
                    const double *eint, const double *cent, const int *nstep, const double *dr, const double *rtab,
                    const double *ptab, const double *ered, int *nodes, int *kfail, int *istat);
+/* MGPROP in the same convention, IMGSEL first. */
+void mgpu_mgprop_f(const int *imgsel, const int *n, const int *nham, const int *nvlblk, const int *ivlfl,
+                   const int *nconst, const int *nrsq, const double *conlen, double *y, const double *vl,
+                   const int *iv, const double *eint, const double *cent, const int *nstep, const double *dr,
+                   const double *rtab, const double *ptab, const double *ered, int *nodes, int *kfail, int *istat);
 
 /* ---- batched propagation plans -----------------------------------------
  * A plan holds many systems and many jobs (one job = one propagation of a

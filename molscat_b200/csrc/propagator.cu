@@ -2319,6 +2319,13 @@ int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered, double 
     return single(MGPU_PROP_LDJ, c, g, ered, z, nodes, kfail);
 }
 
+int mgpu_mgprop(int imgsel, const mgpu_coupling *c, const mgpu_grid *g, double ered, double *y, int *nodes,
+                int *kfail)
+{
+    if (imgsel != 4 && imgsel != 5) return set_err(MGPU_ERR_ARG, "IMGSEL must be 4 (CS4) or 5 (MA5)");
+    return single(imgsel == 4 ? MGPU_PROP_LDMG4 : MGPU_PROP_LDMG5, c, g, ered, y, nodes, kfail);
+}
+
 // Fortran calling convention: every argument by reference, no structures.
 static void single_f(int iprop, const int *n, const int *nham, const int *nvlblk, const int *ivlfl,
                      const int *nconst, const int *nrsq, const double *conlen, double *y, const double *vl,
@@ -2370,6 +2377,20 @@ void mgpu_ldprop_f(const int *n, const int *nham, const int *nvlblk, const int *
 {
     single_f(MGPU_PROP_LDJ, n, nham, nvlblk, ivlfl, nconst, nrsq, conlen, z, vl, iv, eint, cent, nstep, dr, rtab,
              ptab, ered, nodes, kfail, istat);
+}
+
+void mgpu_mgprop_f(const int *imgsel, const int *n, const int *nham, const int *nvlblk, const int *ivlfl,
+                   const int *nconst, const int *nrsq, const double *conlen, double *y, const double *vl,
+                   const int *iv, const double *eint, const double *cent, const int *nstep, const double *dr,
+                   const double *rtab, const double *ptab, const double *ered, int *nodes, int *kfail, int *istat)
+{
+    if (!istat) return;
+    if (!imgsel || (*imgsel != 4 && *imgsel != 5)) {
+        *istat = set_err(MGPU_ERR_ARG, "IMGSEL must be 4 (CS4) or 5 (MA5)");
+        return;
+    }
+    single_f(*imgsel == 4 ? MGPU_PROP_LDMG4 : MGPU_PROP_LDMG5, n, nham, nvlblk, ivlfl, nconst, nrsq, conlen, y, vl,
+             iv, eint, cent, nstep, dr, rtab, ptab, ered, nodes, kfail, istat);
 }
 
 }  // extern "C"

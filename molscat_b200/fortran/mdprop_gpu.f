@@ -1,11 +1,13 @@
-C  Replacements for source_code/mdprop.f and source_code/ldprop.f that
+C  Replacements for source_code/mdprop.f, ldprop.f and mgprop.f that
 C  run the propagation in libmolscat_gpu.so (sm_100a, FP64).  Same
-C  argument lists and meanings as MDPROP (mdprop.f:1-4) and LDPROP
-C  (ldprop.f:1-4); same hidden inputs (module potential, /VLFLAG/,
+C  argument lists and meanings as MDPROP (mdprop.f:1-4), LDPROP
+C  (ldprop.f:1-4) and MGPROP with its MGISEL entry (mgprop.f:1-4,
+C  144-156); same hidden inputs (module potential, /VLFLAG/,
 C  /VLSAVE/, /PRPSCR/); same STOP messages on an inversion failure.
 C
 C  Build: add this file to the Makefile's object list in place of
-C  mdprop.f and ldprop.f and link with -L<dir> -lmolscat_gpu.
+C  mdprop.f, ldprop.f and mgprop.f and link with -L<dir>
+C  -lmolscat_gpu.
 C
 C  What crosses the boundary: the R-dependent half of HAMMAT (POTENL,
 C  the +-1E60 clamp, VCONST, SCAPOT, PERTRB, EP2RU, the 1/R**2 terms;
@@ -119,6 +121,87 @@ C
   901 FORMAT(/' *** ERROR IN SYMINV CALLED FROM LDPROP - TERMINATING')
  1010 FORMAT(/' ***** LDPROP: libmolscat_gpu STATUS ',I3,
      &       ' (include/molscat_gpu.h).  RUN HALTED.')
+      END
+C
+      SUBROUTINE MGPROP(N,MXLAM,NHAM,
+     1                  Y,VL,IV,EINT,CENT,
+     2                  RSTART,RSTOP,NSTEP,DR,NODES,
+     3                  ERED,EP2RU,CM2RU,RSCALE,IPRINT)
+C  IMGSEL (4: CS4, 5: MA5) as set through MGISEL; the stage radii
+C  come from the library (mgpu_ldmg_radii), the P vectors from HAMPVC.
+      USE potential, ONLY: NCONST, NRSQ, NVLBLK, CONLEN
+      USE ISO_C_BINDING, ONLY: C_INT, C_DOUBLE
+      IMPLICIT DOUBLE PRECISION (A-H,O-Z)
+      LOGICAL NOWAVE
+      DIMENSION Y(N,N),VL(*),IV(*),EINT(N),CENT(N)
+      ALLOCATABLE :: RTAB(:),PTAB(:,:),P(:)
+      COMMON /VLFLAG/ IVLFL
+      COMMON /VLSAVE/ IVLU
+      LOGICAL IREAD,IWRITE,IREADR,IWRITR
+      COMMON /PRPSCR/ ESHIFT,ISCRU,ISCRUR,IREAD,IWRITE,IREADR,IWRITR
+      COMMON /MGPUSL/ IMGSLC
+      INTERFACE
+        SUBROUTINE MGPU_MGPROP_F(IMGSEL,N,NHAM,NVLBLK,IVLFL,NCONST,
+     1                           NRSQ,CONLEN,Y,VL,IV,EINT,CENT,NSTEP,
+     2                           DR,RTAB,PTAB,ERED,NODES,KFAIL,ISTAT)
+     3      BIND(C,NAME='mgpu_mgprop_f')
+          USE ISO_C_BINDING, ONLY: C_INT, C_DOUBLE
+          INTEGER(C_INT) IMGSEL,N,NHAM,NVLBLK,IVLFL,NCONST,NRSQ,IV(*),
+     1                   NSTEP,NODES,KFAIL,ISTAT
+          REAL(C_DOUBLE) CONLEN,Y(*),VL(*),EINT(*),CENT(*),DR,
+     1                   RTAB(*),PTAB(*),ERED
+        END SUBROUTINE
+        INTEGER(C_INT) FUNCTION MGPU_LDMG_RADII(IPROP,RSTART,DR,
+     1                                          NSTEP,RTAB)
+     2      BIND(C,NAME='mgpu_ldmg_radii')
+          USE ISO_C_BINDING, ONLY: C_INT, C_DOUBLE
+          INTEGER(C_INT), VALUE :: IPROP,NSTEP
+          REAL(C_DOUBLE), VALUE :: RSTART,DR
+          REAL(C_DOUBLE) RTAB(*)
+        END FUNCTION
+      END INTERFACE
+C
+      NOWAVE=.FALSE.
+      CALL GPUCHK('MGPROP',NOWAVE,IREAD,IWRITE,IVLU,IVLFL,
+     1            MXLAM+NCONST+NRSQ,NHAM)
+      IF (IMGSLC.NE.5) IMGSLC=4
+      IPROP=80+IMGSLC
+      NP=MAX(NHAM,1)
+      NR=MAX(4*NSTEP+1,6*NSTEP)
+      ALLOCATE (RTAB(NR),PTAB(NP,NR))
+      ALLOCATE (P(MAX(MXLAM+NCONST+NRSQ,NHAM,1)))
+      NR=MGPU_LDMG_RADII(IPROP,RSTART,DR,NSTEP,RTAB)
+      DO K=1,NR
+        P=0.D0
+        CALL HAMPVC(RTAB(K),P,MXLAM,EP2RU,CM2RU,RSCALE,IPRINT)
+        DO I=1,NHAM
+          PTAB(I,K)=P(I)
+        ENDDO
+      ENDDO
+      CALL MGPU_MGPROP_F(IMGSLC,N,NHAM,NVLBLK,IVLFL,NCONST,NRSQ,
+     1                   CONLEN,Y,VL,IV,EINT,CENT,NSTEP,DR,RTAB,PTAB,
+     2                   ERED,NODES,KFAIL,ISTAT)
+      DEALLOCATE (RTAB,PTAB,P)
+      IF (ISTAT.NE.0) THEN
+        WRITE(6,1010) ISTAT,KFAIL
+        STOP
+      ENDIF
+      RETURN
+ 1010 FORMAT(/' ***** MGPROP: libmolscat_gpu STATUS ',I3,
+     &       ' IN SECTOR ',I6,' (include/molscat_gpu.h).  RUN HALTED.')
+      END
+C
+      SUBROUTINE MGISEL(IMGSEL)
+C  The MGPROP method: 4 (CS4) or 5 (MA5), as mgprop.f:144-156.
+      COMMON /MGPUSL/ IMGSLC
+      IF (IMGSEL.EQ.4 .OR. IMGSEL.EQ.5) THEN
+        IMGSLC=IMGSEL
+      ELSE
+        WRITE(6,*) ' *** ERROR *** ONLY CS4 AND MA5 SYMPLECTIC '//
+     1             'PROPAGATORS CODED AT THE MOMENT'
+        STOP
+      ENDIF
+      RETURN
       END
 C
       SUBROUTINE GPUCHK(NAME,WAVE,IREAD,IWRITE,IVLU,IVLFL,NPTOT,NHAM)

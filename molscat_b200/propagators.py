@@ -169,6 +169,8 @@ def _raise_for(name: str, status: int, step: int):
     if status == _lib.MGPU_ERR_INVERSION or status == _lib.MGPU_ERR_NONFINITE:
         if name == "MDPROP":
             msg = f" ***** MDPROP: MATRIX INVERSION ERROR AT STEP K = {step:6d}.  RUN HALTED."
+        elif name == "MGPROP":
+            msg = f" MGPROP: MATRIX INVERSION ERROR IN SECTOR {step:6d}"
         else:
             msg = " *** ERROR IN SYMINV CALLED FROM LDPROP - TERMINATING"
         if status == _lib.MGPU_ERR_NONFINITE:
@@ -187,19 +189,23 @@ def _single(name, iprop, coupling: Coupling, seg: Segment, ered: float, y0: np.n
     g = seg.c_struct()
     nodes = ctypes.c_int(0)
     kfail = ctypes.c_int(0)
-    fn = L.mgpu_mdprop if iprop == MGPU_PROP_LDMD else L.mgpu_ldprop
-    rc = fn(ctypes.byref(c), ctypes.byref(g), float(ered), y.ctypes.data_as(_dp),
-            ctypes.byref(nodes), ctypes.byref(kfail))
+    if iprop in (MGPU_PROP_LDMG4, MGPU_PROP_LDMG5):
+        rc = L.mgpu_mgprop(4 if iprop == MGPU_PROP_LDMG4 else 5, ctypes.byref(c), ctypes.byref(g), float(ered),
+                           y.ctypes.data_as(_dp), ctypes.byref(nodes), ctypes.byref(kfail))
+    else:
+        fn = L.mgpu_mdprop if iprop == MGPU_PROP_LDMD else L.mgpu_ldprop
+        rc = fn(ctypes.byref(c), ctypes.byref(g), float(ered), y.ctypes.data_as(_dp),
+                ctypes.byref(nodes), ctypes.byref(kfail))
     if rc != 0:
         _raise_for(name, rc, kfail.value)
     return y, nodes.value
 
 
 def _args_to_inputs(n, mxlam, nham, vl, iv, eint, cent, rstart, rstop, nstep, dr, potential, nvlblk, ivlfl,
-                    nconst, nrsq, conlen):
+                    nconst, nrsq, conlen, kind="LD"):
     coupling = Coupling(n=n, nham=nham, vl=vl, eint=eint, cent=cent, nvlblk=nvlblk or nham, iv=iv,
                         ivlfl=ivlfl, nconst=nconst, nrsq=nrsq, conlen=conlen)
-    seg = Segment.build(rstart, dr, nstep, potential, nham)
+    seg = Segment.build(rstart, dr, nstep, potential, nham, kind=kind)
     return coupling, seg
 
 
@@ -223,12 +229,31 @@ def ldprop(n, mxlam, nham, z, vl, iv, eint, cent, rstart, rstop, nstep, dr, ered
     return _single("LDPROP", MGPU_PROP_LDJ, coupling, seg, ered, z)
 
 
+def mgprop(n, mxlam, nham, y, vl, iv, eint, cent, rstart, rstop, nstep, dr, ered, *, potential, imgsel=4,
+           nvlblk=0, ivlfl=0, nconst=0, nrsq=0, conlen=0.0):
+    """MGPROP (mgprop.f:1-134) on the GPU, IMGSEL = 4 (CS4) or 5 (MA5):
+    NSTEP sectors of DR from RSTART; ``potential(r)`` as for :func:`mdprop`,
+    evaluated at every stage's radius.  Returns (Y at RSTOP, NODES)."""
+    del mxlam, rstop
+    if imgsel not in (4, 5):
+        raise ValueError("IMGSEL must be 4 (CS4) or 5 (MA5)")
+    kind = f"LDMG{imgsel}"
+    coupling, seg = _args_to_inputs(n, 0, nham, vl, iv, eint, cent, rstart, None, nstep, dr, potential, nvlblk,
+                                    ivlfl, nconst, nrsq, conlen, kind=kind)
+    return _single("MGPROP", PROPS[kind], coupling, seg, ered, y)
+
+
 def propagate(prop: str, coupling: Coupling, seg: Segment, ered: float, y0: np.ndarray):
-    """One propagation from prepared inputs: prop is "LDMD" or "LDJ"."""
+    """One propagation from prepared inputs: prop is "LDMD", "LDJ", "LDMG4" or
+    "LDMG5" (the segment of the matching kind)."""
     if prop == "LDMD":
         return _single("MDPROP", MGPU_PROP_LDMD, coupling, seg, ered, y0)
     if prop == "LDJ":
         return _single("LDPROP", MGPU_PROP_LDJ, coupling, seg, ered, y0)
+    if prop in ("LDMG4", "LDMG5"):
+        if seg.kind != prop:
+            raise ValueError(f"{prop} needs a {prop} segment")
+        return _single("MGPROP", PROPS[prop], coupling, seg, ered, y0)
     raise ValueError(prop)
 
 

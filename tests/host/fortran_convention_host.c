@@ -1,7 +1,7 @@
 /*
  * A test host that calls libmolscat_gpu the way a Fortran caller does:
  * the replacement MDPROP/LDPROP in molscat_b200/fortran/mdprop_gpu.f binds
- * mgpu_mdprop_f / mgpu_ldprop_f through a BIND(C) interface block without
+ * mgpu_mdprop_f / mgpu_ldprop_f / mgpu_mgprop_f through a BIND(C) interface block without
  * VALUE attributes, so every scalar arrives as the address of a variable
  * and every array as the address of its first element, column-major.
  *
@@ -44,7 +44,8 @@ int main(int argc, char **argv)
         nrsq = hdr[6], nstep = hdr[7];
     double conlen = hd[0], dr = hd[1], ered = hd[2];
     const size_t npair = n > 0 ? (size_t)n * (n + 1) / 2 : 0, nn = n > 0 ? (size_t)n * n : 0;
-    const size_t nr = nstep > 0 ? 2 * (size_t)nstep + 1 : 0;
+    const int ldmg = iprop == MGPU_PROP_LDMG4 || iprop == MGPU_PROP_LDMG5;
+    const size_t nr = nstep < 1 ? 0 : ldmg ? (size_t)mgpu_ldmg_radii(iprop, 0.0, 1.0, nstep, NULL) : 2 * (size_t)nstep + 1;
     double *vl = take(f, sizeof(double) * nvlblk * npair);
     int *iv = take(f, sizeof(int) * nvlblk * npair);
     double *eint = take(f, sizeof(double) * (n > 0 ? n : 0));
@@ -55,9 +56,13 @@ int main(int argc, char **argv)
     fclose(f);
 
     int nodes = -1, kfail = -1, istat = -1;
+    int imgsel = iprop == MGPU_PROP_LDMG5 ? 5 : 4;
     if (iprop == MGPU_PROP_LDMD)
         mgpu_mdprop_f(&n, &nham, &nvlblk, &ivlfl, &nconst, &nrsq, &conlen, y, vl, iv, eint, cent, &nstep, &dr, rtab,
                       ptab, &ered, &nodes, &kfail, &istat);
+    else if (ldmg)
+        mgpu_mgprop_f(&imgsel, &n, &nham, &nvlblk, &ivlfl, &nconst, &nrsq, &conlen, y, vl, iv, eint, cent, &nstep,
+                      &dr, rtab, ptab, &ered, &nodes, &kfail, &istat);
     else
         mgpu_ldprop_f(&n, &nham, &nvlblk, &ivlfl, &nconst, &nrsq, &conlen, y, vl, iv, eint, cent, &nstep, &dr, rtab,
                       ptab, &ered, &nodes, &kfail, &istat);

@@ -1,8 +1,9 @@
 """The Fortran calling convention at the boundary.
 
-The replacement MDPROP/LDPROP (molscat_b200/fortran/mdprop_gpu.f) binds
-mgpu_mdprop_f / mgpu_ldprop_f with a plain BIND(C) interface block, every
-argument by reference.  No Fortran compiler exists in this image, so a C
+The replacement MDPROP/LDPROP/MGPROP (molscat_b200/fortran/mdprop_gpu.f)
+binds mgpu_mdprop_f / mgpu_ldprop_f / mgpu_mgprop_f (and mgpu_ldmg_radii for
+MGPROP's stage radii) with plain BIND(C) interface blocks, every argument
+by reference except the radii helper's scalars.  No Fortran compiler exists in this image, so a C
 host (tests/host/fortran_convention_host.c) makes the same calls: each
 scalar as the address of a variable, each array column-major.
 
@@ -10,7 +11,8 @@ scalar as the address of a variable, each array column-major.
   MGPU_ERR_ARG back for a bad step (no GPU needed for argument checks); the
   shim source declares the two entry points the header declares.
 * GPU: the host's results equal the Python path's (the C ABI through
-  ctypes) bit for bit, MDPROP and LDPROP, with IV indexing.
+  ctypes) bit for bit, MDPROP and LDPROP with IV indexing, MGPROP (CS4 and
+  MA5) on the one-warp and one-CTA kernels.
 """
 import os
 import re
@@ -66,8 +68,8 @@ def test_shim_binds_the_declared_entry_points():
     with open(os.path.join(ROOT, "molscat_b200", "fortran", "mdprop_gpu.f")) as f:
         src = f.read()
     names = set(re.findall(r"NAME='(mgpu_[a-z_]+)'", src))
-    assert names == {"mgpu_mdprop_f", "mgpu_ldprop_f"}
-    assert {"mgpu_mdprop_f", "mgpu_ldprop_f"} <= set(_lib.EXPORTS)
+    assert names == {"mgpu_mdprop_f", "mgpu_ldprop_f", "mgpu_mgprop_f", "mgpu_ldmg_radii"}
+    assert names <= set(_lib.EXPORTS)
     for ln in src.splitlines():  # fixed form: statements end by column 72
         assert ln[:1] in "Cc" or len(ln) <= 72, ln
 
@@ -92,5 +94,21 @@ def test_host_matches_python_path(host, tmp_path, iprop, n, kw):
     istat, nodes, kfail, y = _run(host, tmp_path, iprop, c, seg, ered, y0)
     assert istat == 0 and kfail == 0
     yp, np_ = propagate("LDMD" if iprop == 6 else "LDJ", c, seg, ered, y0)
+    assert nodes == np_
+    assert np.array_equal(y, yp)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["LDMG4", "LDMG5"])
+@pytest.mark.parametrize("n", [12, 36, 70])
+def test_host_matches_python_path_mgprop(host, tmp_path, kind, n):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from molscat_b200.propagators import PROPS, propagate
+    c, seg, ered, y0 = cases.random_case(n, 60, seed=400 + n, kind=kind)
+    istat, nodes, kfail, y = _run(host, tmp_path, PROPS[kind], c, seg, ered, y0)
+    assert istat == 0 and kfail == 0
+    yp, np_ = propagate(kind, c, seg, ered, y0)
     assert nodes == np_
     assert np.array_equal(y, yp)

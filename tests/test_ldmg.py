@@ -91,6 +91,22 @@ def test_gpu_random_systems_match_oracle(gpu, kind, n):
 
 
 @pytest.mark.gpu
+def test_gpu_single_call_equals_plan(gpu):
+    """mgpu_mgprop (the MGPROP drop-in, Python mgprop with MGPROP's argument
+    list) gives the plan's result bit for bit."""
+    from molscat_b200.propagators import mgprop, propagate
+    c, seg, ered, y0 = cases.random_case(20, 50, seed=9, kind="LDMG5")
+    plan = Plan("LDMG5", [c], [seg], np.zeros(1, dtype=np.int32), np.array([ered]))
+    ybuf, nodes, status, _ = plan.run_host(plan.pack([y0]))
+    ys, ns = propagate("LDMG5", c, seg, ered, y0)
+    yf, nf = mgprop(c.n, c.nham, c.nham, y0, c.vl, None, c.eint, c.cent, float(seg.rtab[0]), None, 50, seg.dr,
+                    ered, potential=seg.pvec, imgsel=5)
+    assert np.array_equal(plan.unpack(ybuf, 0), ys) and np.array_equal(ys, yf)
+    assert nodes[0] == ns == nf
+    plan.close()
+
+
+@pytest.mark.gpu
 def test_gpu_refuses_n_above_200(gpu):
     from molscat_b200.propagators import PropagatorError
     c, seg, ered, y0 = cases.random_case(201, 2, seed=5, kind="LDMG4")
