@@ -59,7 +59,7 @@ extern "C" {
 /* MGPROP (mgprop.f:1-134): the symplectic log-derivative propagator of
  * Manolopoulos and Gray, the reference's IPROP = 8 with IMGSEL = 4 (CS4,
  * five stages, four inversions a sector) or 5 (MA5, six stages and
- * inversions).  Plans only, N <= 200 (the one-warp and one-CTA kernels).  Its grid's
+ * inversions).  N <= 1024 (the one-warp, one-CTA and large-N families).  Its grid's
  * NSTEP is the number of sectors of width DR, and RTAB/PTAB list the radii
  * where the stages evaluate W, in order (mgpu_ldmg_radii): 4*NSTEP + 1 rows
  * for CS4, 6*NSTEP for MA5. */
@@ -102,7 +102,7 @@ int mgpu_ldprop(const mgpu_coupling *c, const mgpu_grid *g, double ered,
                 double *z, int *nodes, int *kfail);
 /* mgpu_mgprop replaces MGPROP (mgprop.f:1-134) with IMGSEL = 4 (CS4) or 5
  * (MA5): g's tables are the stage radii of mgpu_ldmg_radii; y in and out
- * as MGPROP's Y.  N <= 200. */
+ * as MGPROP's Y.  N <= 1024. */
 int mgpu_mgprop(int imgsel, const mgpu_coupling *c, const mgpu_grid *g, double ered,
                 double *y, int *nodes, int *kfail);
 

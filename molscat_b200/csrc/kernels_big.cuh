@@ -721,11 +721,81 @@ __global__ void __launch_bounds__(EW_THREADS) big_ldj_post_kernel(StepArgs a)
     }
 }
 
-// Results: Y = tiles/H (MDPROP, mdprop.f:269-275) or Z/H - I/H (LDPROP,
-// ldprop.f:140-147) into the caller's column-major Y, both triangles;
-// NODES (MDPROP: minus the U(C) count NSAVE), status and failing step.
+// MGPROP start: the tiles hold Y0 (mgprop.f:63), the counters cleared.
+__global__ void __launch_bounds__(EW_THREADS) big_ldmg_init_kernel(StepArgs a, const double *__restrict__ y)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *md.cnt = 0;
+        *md.stat = 0;
+        *md.kfail = INT_MAX;
+    }
+    const double *yj = y + job.yoff;
+    const int n = S.n;
+    for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        elem_ij(x, i, j);
+        const int lo = i < j ? i : j, hi = i < j ? j : i;
+        md.a[x] = (i < n && j < n) ? yj[(size_t)lo * n + hi] : 0.0;
+    }
+}
+
+// MGPROP stage k of sector kstep (mgprop.f:94-104): X = Y + b_k h W(R) at
+// radius row (kstep-1)*stride + k, then for a_k != 0 the matrix to invert,
+// I + a_k h X (a_k = 0: Y = X); h is the matrix's own sector width.
+__global__ void __launch_bounds__(EW_THREADS) big_ldmg_stage_kernel(StepArgs a, int stride, int k, double bk, double ak)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    const int ks = *a.kstep;
+    if (ks > md.nstep) return;
+    const double bh = bk * S.dr, ah = ak * S.dr;
+    const int ir = (ks - 1) * stride + k;
+    const double *P = ptab_row(S, ir);
+    double2 *yv = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        pair_ij(p, i, j);
+        const double2 w = w_pair(S, P, p, i, j, ir, job.ered), yp = yv[p];
+        double x0 = fma(bh, w.x, yp.x), x1 = fma(bh, w.y, yp.y);
+        if (ah != 0.0) {
+            x0 = ah * x0 + ((i == j && i < S.n) ? 1.0 : 0.0);
+            x1 = ah * x1 + ((i == j + 1 && i < S.n) ? 1.0 : 0.0);
+        }
+        yv[p] = make_double2(x0, x1);
+    }
+}
+
+// After the inversion (the tiles hold -(I + a_k h X)^-1): Y = [I - inverse]/(a_k h)
+__global__ void __launch_bounds__(EW_THREADS) big_ldmg_after_kernel(StepArgs a, double ak)
+{
+    const int m = blockIdx.y;
+    const JobDev job = a.jobs[m];
+    const SysDev S = a.sys[job.sys];
+    const MatDesc md = a.md[m];
+    if (*a.kstep > md.nstep) return;
+    const double d1 = 1.0 / (ak * S.dr);
+    double2 *yv = reinterpret_cast<double2 *>(md.a);
+    for (size_t p = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; p < a.td / 2; p += (size_t)gridDim.x * EW_THREADS) {
+        int i, j;
+        pair_ij(p, i, j);
+        const double2 yp = yv[p];
+        yv[p] = make_double2((yp.x + ((i == j && i < S.n) ? 1.0 : 0.0)) * d1,
+                             (yp.y + ((i == j + 1 && i < S.n) ? 1.0 : 0.0)) * d1);
+    }
+}
+
+// Results: Y = tiles/H (MDPROP, mdprop.f:269-275), Z/H - I/H (LDPROP,
+// ldprop.f:140-147) or the tiles as they are (MGPROP) into the caller's
+// column-major Y, both triangles; NODES (MDPROP: minus the U(C) count
+// NSAVE), status and failing step.  mode: 0 MDPROP, 1 LDPROP, 2 MGPROP.
 __global__ void __launch_bounds__(EW_THREADS)
-big_finish_kernel(StepArgs a, int ldj, double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
+big_finish_kernel(StepArgs a, int mode, double *__restrict__ y, int *__restrict__ nodes_out, int *__restrict__ status_out,
                   int *__restrict__ kfail_out)
 {
     const int m = blockIdx.y;
@@ -736,10 +806,11 @@ big_finish_kernel(StepArgs a, int ldj, double *__restrict__ y, int *__restrict__
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         status_out[job.out] = st;
         kfail_out[job.out] = st ? *md.kfail : 0;
-        nodes_out[job.out] = st ? 0 : (*md.cnt - (ldj ? 0 : S.prep[0]));
+        nodes_out[job.out] = st ? 0 : (*md.cnt - (mode == 0 ? S.prep[0] : 0));
     }
     if (st) return;
-    const double hi = 2.0 / S.dr;
+    const bool ldj = mode == 1;
+    const double hi = mode == 2 ? 1.0 : 2.0 / S.dr;
     const int n = S.n;
     double *yj = y + job.yoff;
     for (size_t x = (size_t)blockIdx.x * EW_THREADS + threadIdx.x; x < a.td; x += (size_t)gridDim.x * EW_THREADS) {

@@ -674,10 +674,10 @@ static size_t matrix_elems(int b) { return tile_elems(b) * ntiles_of(b); }      
 // LDJ keeps two tiled matrices in shared memory: CTA buckets up to N = 128.
 static bool is_ldmg(int iprop) { return iprop == MGPU_PROP_LDMG4 || iprop == MGPU_PROP_LDMG5; }
 
-// LDMG runs on the one-warp and one-CTA kernels (N <= 200).
+// LDMG runs on the fragment-layout families: one warp, one CTA, batched large N.
 static bool bucket_allows(int b, int iprop)
 {
-    if (is_ldmg(iprop)) return kBuckets[b].kind == KIND_FRAG8 || kBuckets[b].kind == KIND_CTA8;
+    if (is_ldmg(iprop)) return kBuckets[b].kind != KIND_TILE4;
     return !(iprop == MGPU_PROP_LDJ && kBuckets[b].kind == KIND_CTA8 && kBuckets[b].nt > 16);
 }
 
@@ -954,7 +954,7 @@ struct BigBucket {
     int M = 0;                            // jobs
     const JobDev *d_jobs = nullptr;       // this bucket's jobs
     big::MatDesc *d_md = nullptr;         // per job: Y (MDPROP) or Z (LDPROP)
-    big::MatDesc *d_mduz = nullptr;       // LDPROP: [U of every job, Z of every job]
+    big::MatDesc *d_mduz = nullptr;       // LDPROP: [U of every job, Z of every job]; MGPROP: Y counted with sign -1
     double *tiles = nullptr, *tiles2 = nullptr, *vec = nullptr;
     int *ctr = nullptr;                   // [3][M]: pivot count, status, failing step
     big::Panels pn[2]{};                  // shared Lam / 1/delta, X and B twice
@@ -1290,7 +1290,7 @@ static int setup_big(BigBucket &g, int iprop, int b, const JobDev *jobs, const J
         (e = put_n(al, up, &g.kzero, &zero, 1)) ||
         (M && ((e = alloc_n(al, &g.tiles, (size_t)M * g.td)) || (e = alloc_n(al, &g.ctr, (size_t)3 * M)) ||
                (ldj && (e = alloc_n(al, &g.tiles2, (size_t)M * g.td))) ||
-               (!ldj && (e = alloc_n(al, &g.vec, (size_t)M * 3 * g.npad))))))
+               (iprop == MGPU_PROP_LDMD && (e = alloc_n(al, &g.vec, (size_t)M * 3 * g.npad))))))
         return set_err(MGPU_ERR_NOMEM, "allocating large-N matrices", e);
     g.pn[1].lam = g.pn[0].lam;
     g.pn[1].rd = g.pn[0].rd;
@@ -1314,9 +1314,12 @@ static int setup_big(BigBucket &g, int iprop, int b, const JobDev *jobs, const J
                 uz[j].sign = -1;
             }
             uz.insert(uz.end(), md.begin(), md.end());
+        } else if (is_ldmg(iprop)) {
+            uz = md;  // the same matrices counted with sign -1: MGPROP's stages with a_k < 0
+            for (int j = 0; j < M; ++j) uz[j].sign = -1;
         }
         if ((e = put_n(al, up, &g.d_md, md.data(), md.size())) ||
-            (ldj && (e = put_n(al, up, &g.d_mduz, uz.data(), uz.size()))))
+            (!uz.empty() && (e = put_n(al, up, &g.d_mduz, uz.data(), uz.size()))))
             return set_err(MGPU_ERR_NOMEM, "uploading large-N descriptors", e);
     }
     if (!ldj)
@@ -1379,7 +1382,17 @@ static cudaError_t run_big_prop(BigBucket &g, int iprop, const SysDev *d_sys, do
     const dim3 ew(big_ew_blocks(g.td), g.M), ev((g.npad + big::EW_THREADS - 1) / big::EW_THREADS, g.M);
     auto one_step = [&]() -> cudaError_t {
         cudaError_t x;
-        if (ldj) {
+        if (is_ldmg(iprop)) {
+            // one sector: the stages of mgprop.f:75-131 with the coefficients of the method
+            const wf::MGCoef &mc = wf::kMGCoef[iprop == MGPU_PROP_LDMG5 ? 1 : 0];
+            for (int k = 0; k < mc.m; ++k) {
+                big::big_ldmg_stage_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, mc.stride, k, mc.b[k], mc.a[k]);
+                if (mc.a[k] == 0.0) continue;
+                if ((x = big_invert(mc.a[k] >= 0.0 ? g.d_md : g.d_mduz, g.M, g.nt, g.pn, g.kstep, st, side, evf, evj)))
+                    return x;
+                big::big_ldmg_after_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, mc.a[k]);
+            }
+        } else if (ldj) {
             big::big_ldj_pre_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
             if ((x = big_invert(g.d_mduz, 2 * g.M, g.nt, g.pn, g.kstep, st, side, evf, evj))) return x;  // U and Z
             big::big_ldj_mid_kernel<<<ew, big::EW_THREADS, 0, st>>>(a);
@@ -1412,11 +1425,13 @@ static cudaError_t run_big_prop(BigBucket &g, int iprop, const SysDev *d_sys, do
         }
     }
     big::big_step_advance_kernel<<<1, 1, 0, st>>>(g.kstep, 1);
-    if (ldj) big::big_ldj_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
+    if (is_ldmg(iprop)) big::big_ldmg_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
+    else if (ldj) big::big_ldj_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
     else big::big_ldmd_init_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, y);
     for (int k = 1; k <= g.max_nstep; ++k)
         if ((e = cudaGraphLaunch(g.step_graph, st))) return e;
-    big::big_finish_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, ldj ? 1 : 0, y, nodes, status, kfail);
+    big::big_finish_kernel<<<ew, big::EW_THREADS, 0, st>>>(a, is_ldmg(iprop) ? 2 : (ldj ? 1 : 0), y, nodes, status,
+                                                            kfail);
     return cudaGetLastError();
 }
 
@@ -1618,7 +1633,17 @@ int mgpu_plan_launches(const mgpu_plan *p)
                 const int chunks = (ns + g.pcap - 1) / g.pcap;
                 l += chunks * (2 + per_inv);
             }
-        if (g.M > 0) l += 3 + g.max_nstep * (4 + 2 * per_inv);
+        if (g.M > 0) {
+            int per_step = 4 + 2 * per_inv;  // MDPROP: three elementwise kernels, two inversions, the counter
+            if (p->iprop == MGPU_PROP_LDJ) {
+                per_step = 4 + 2 * per_inv;
+            } else if (is_ldmg(p->iprop)) {
+                const wf::MGCoef &mc = wf::kMGCoef[p->iprop == MGPU_PROP_LDMG5 ? 1 : 0];
+                per_step = 1;
+                for (int k = 0; k < mc.m; ++k) per_step += 1 + (mc.a[k] != 0.0 ? 1 + per_inv : 0);
+            }
+            l += 3 + g.max_nstep * per_step;
+        }
     }
     return l;
 }
@@ -1717,8 +1742,6 @@ int mgpu_plan_create(mgpu_plan **out, int iprop, int nsys, const mgpu_coupling *
     if (nsys < 1 || njobs < 0 || !systems || !grids || (njobs > 0 && (!job_sys || !job_ered)))
         return set_err(MGPU_ERR_ARG, "bad system/job arrays");
     for (int s = 0; s < nsys; ++s) {
-        if (is_ldmg(iprop) && systems[s].n > 200)
-            return set_err(MGPU_ERR_UNSUPPORTED, "LDMG runs on the one-warp and one-CTA kernels: N <= 200");
         int rc = check_coupling(&systems[s], &grids[s], iprop);
         if (rc) return rc;
     }

@@ -1,6 +1,6 @@
 """MGPROP, the symplectic log-derivative propagator (mgprop.f; the
 reference's IPROP = 8 with IMGSEL = 4 (CS4) or 5 (MA5)), on the one-warp
-(N <= 40) and one-CTA (N <= 200) kernels against the oracle's restatement
+(N <= 40), one-CTA (N <= 200) and batched large-N kernels against the oracle's restatement
 (oracle/oracle.py, mgprop), which reproduces the reference's MA5 S
 matrices of molscat-all_propagators (tests/test_oracle_golden.py, 3.5e-12).
 
@@ -9,9 +9,8 @@ matrices of molscat-all_propagators (tests/test_oracle_golden.py, 3.5e-12).
   bit, with CS4's last-stage reuse; a plan rejects a segment of the wrong
   kind.
 * GPU: the reference's golden S matrices (N = 12, 8072 sectors, both
-  energies) with the GPU propagating; random systems N = 5..150 for CS4 and
-  MA5 against the oracle (Y within 5e-8 of max|Y|, NODES exact); N > 200
-  refused.
+  energies) with the GPU propagating; random systems N = 5..300 for CS4 and
+  MA5 against the oracle (Y within 5e-8 of max|Y|, NODES exact).
 """
 import numpy as np
 import pytest
@@ -107,11 +106,25 @@ def test_gpu_single_call_equals_plan(gpu):
 
 
 @pytest.mark.gpu
-def test_gpu_refuses_n_above_200(gpu):
-    from molscat_b200.propagators import PropagatorError
-    c, seg, ered, y0 = cases.random_case(201, 2, seed=5, kind="LDMG4")
-    with pytest.raises(PropagatorError):
-        Plan("LDMG4", [c], [seg], np.zeros(1, dtype=np.int32), np.array([ered]))
+@pytest.mark.parametrize("kind", ["LDMG4", "LDMG5"])
+@pytest.mark.parametrize("n", [212, 300])
+def test_gpu_large_n_matches_oracle(gpu, kind, n):
+    """N > 200: the batched large-N kernels (64-pivot rounds), the stages as
+    elementwise kernels between the inversions, a_k < 0 stages counted with
+    sign -1."""
+    from oracle import oracle as O
+    nstep = 12
+    c, seg, ered, y0 = cases.random_case(n, nstep, seed=80 + n, kind=kind)
+    erg = ered + np.array([0.0, 2.0])
+    plan = Plan(kind, [c], [seg], np.zeros(2, dtype=np.int32), erg)
+    ybuf, nodes, status, _ = plan.run_host(plan.pack([y0, y0]))
+    assert (status == 0).all()
+    oc = cases.to_oracle(c)
+    for j, e in enumerate(erg):
+        yo, no = O.mgprop(oc, _Pot(seg.pvec), float(seg.rtab[0]), seg.dr, nstep, float(e), y0, int(kind[-1]))
+        assert nodes[j] == no
+        assert np.abs(plan.unpack(ybuf, j) - yo).max() <= 5e-8 * np.abs(yo).max()
+    plan.close()
 
 
 @pytest.mark.gpu
