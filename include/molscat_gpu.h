@@ -182,6 +182,24 @@ int mgpu_plan_run_device_phases(mgpu_plan *plan, double *y_dev, int *nodes_dev,
                                 int *status_dev, int *kfail_dev, void *stream,
                                 int phases);
 
+/* ---- MAPROP (LDMA) ----------------------------------------------------------
+ * The quasi-adiabatic log-derivative propagator (maprop.f:1-290, IPROP = 7)
+ * for many energies of one system, N <= 64.  Its energy-independent half --
+ * per sector k the eigenvalues EIVAL of W at the midpoint (with ERED = 0),
+ * the basis change Q_k = T_{k-1}^T U_k and the first-order correction C_k
+ * in the old basis, then the last basis T and end correction Q_end -- is
+ * built on the host once per system (what the reference keeps on its ISCRU
+ * file after the first energy; molscat_b200.ldma builds them).  Tables:
+ * eival[nstep][n], q[nstep][n*n], corr[nstep][n*n], tfin[n*n], qfin[n*n],
+ * matrices column-major.  inward != 0 for DR < 0 (a sector adds N - count).
+ * mgpu_ldma_run_host: y[njobs][n*n] in (the initial Y in the primitive
+ * basis) and out (Y at the end), nodes and status per job. */
+typedef struct mgpu_ldma mgpu_ldma;
+int mgpu_ldma_create(mgpu_ldma **out, int n, int nstep, double dr, int inward, const double *eival,
+                     const double *q, const double *corr, const double *tfin, const double *qfin);
+int mgpu_ldma_run_host(mgpu_ldma *h, int njobs, const double *ered, double *y, int *nodes, int *status);
+void mgpu_ldma_destroy(mgpu_ldma *h);
+
 /* ---- Y -> K -> S on the device ---------------------------------------------
  * YTOK/YTOKG/KSYM (ytok.f:21-47, ytokg.f:71-126) and KTOS (ktos.f:149-169)
  * for every job after its propagation, at R = the grid's last radius: the

@@ -2628,4 +2628,96 @@ extern "C" int mgpu_mdprop_noalloc(const mgpu_coupling *c, const mgpu_grid *g, i
         return set_err(MGPU_ERR_CUDA, "launching ldmd_prop_kernel", e);
     return MGPU_OK;
 }
+#include "kernels_ldma.cuh"
+
+// ---- MAPROP for the energies of one system (tables from the host) --------
+struct mgpu_ldma {
+    mgpu::ldma::Tables t{};
+    std::vector<void *> allocs;
+    cudaStream_t own = nullptr;
+    ~mgpu_ldma()
+    {
+        if (own) cudaStreamSynchronize(own);
+        for (void *p : allocs) cudaFree(p);
+        if (own) cudaStreamDestroy(own);
+    }
+};
+
+extern "C" int mgpu_ldma_create(mgpu_ldma **out, int n, int nstep, double dr, int inward, const double *eival,
+                                const double *q, const double *corr, const double *tfin, const double *qfin)
+{
+    if (!out) return set_err(MGPU_ERR_ARG, "null handle pointer");
+    *out = nullptr;
+    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "LDMA runs for 1 <= N <= 64");
+    if (nstep < 1 || !(dr != 0.0) || !std::isfinite(dr)) return set_err(MGPU_ERR_ARG, "bad NSTEP or DR");
+    if (!eival || !q || !corr || !tfin || !qfin) return set_err(MGPU_ERR_ARG, "null table");
+    mgpu_ldma *h = new (std::nothrow) mgpu_ldma();
+    if (!h) return set_err(MGPU_ERR_NOMEM, "host allocation failed");
+    const size_t nn = (size_t)n * n;
+    const AllocFn al = [h](void **p, size_t nb) {
+        cudaError_t e = cudaMalloc(p, nb);
+        if (e == cudaSuccess) h->allocs.push_back(*p);
+        return e;
+    };
+    const UploadFn up = [](void *dst, const void *src, size_t nb) {
+        return cudaMemcpy(dst, src, nb, cudaMemcpyHostToDevice);
+    };
+    double *de = nullptr, *dq = nullptr, *dc = nullptr, *dt = nullptr, *dqf = nullptr;
+    cudaError_t e;
+    if ((e = put_n(al, up, &de, eival, (size_t)nstep * n)) || (e = put_n(al, up, &dq, q, (size_t)nstep * nn)) ||
+        (e = put_n(al, up, &dc, corr, (size_t)nstep * nn)) || (e = put_n(al, up, &dt, tfin, nn)) ||
+        (e = put_n(al, up, &dqf, qfin, nn)) || (e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking))) {
+        delete h;
+        return set_err(MGPU_ERR_NOMEM, "uploading the LDMA tables", e);
+    }
+    h->t = mgpu::ldma::Tables{n, nstep, inward ? 1 : 0, dr, de, dq, dc, dt, dqf};
+    *out = h;
+    return MGPU_OK;
+}
+
+extern "C" int mgpu_ldma_run_host(mgpu_ldma *h, int njobs, const double *ered, double *y, int *nodes, int *status)
+{
+    if (!h) return set_err(MGPU_ERR_ARG, "null handle");
+    if (njobs < 0 || njobs > 65535) return set_err(MGPU_ERR_ARG, "0 <= jobs <= 65535");
+    if (njobs == 0) return MGPU_OK;
+    if (!ered || !y || !nodes || !status) return set_err(MGPU_ERR_ARG, "null host buffer");
+    for (int j = 0; j < njobs; ++j)
+        if (!std::isfinite(ered[j])) return set_err(MGPU_ERR_ARG, "ERED not finite");
+    const size_t nn = (size_t)h->t.n * h->t.n;
+    double *de = nullptr, *dy = nullptr;
+    int *dn = nullptr, *ds = nullptr;
+    cudaError_t e;
+    cudaStream_t st = h->own;
+    if ((e = cudaMallocAsync((void **)&de, njobs * sizeof(double), st)) ||
+        (e = cudaMallocAsync((void **)&dy, njobs * nn * sizeof(double), st)) ||
+        (e = cudaMallocAsync((void **)&dn, njobs * sizeof(int), st)) ||
+        (e = cudaMallocAsync((void **)&ds, njobs * sizeof(int), st)))
+        return set_err(MGPU_ERR_NOMEM, "LDMA buffers", e);
+    int rc = MGPU_OK;
+    if ((e = cudaMemcpyAsync(de, ered, njobs * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(dy, y, njobs * nn * sizeof(double), cudaMemcpyHostToDevice, st)))
+        rc = set_err(MGPU_ERR_CUDA, "copying LDMA inputs", e);
+    if (!rc) {
+        const size_t sm = mgpu::ldma::smem_bytes(h->t.n);
+        if ((e = set_smem(mgpu::ldma::ldma_kernel, sm))) {
+            rc = set_err(MGPU_ERR_CUDA, "ldma_kernel set-up", e);
+        } else {
+            mgpu::ldma::ldma_kernel<<<njobs, mgpu::ldma::kThreads, sm, st>>>(h->t, de, dy, dn, ds);
+            if ((e = cudaGetLastError())) rc = set_err(MGPU_ERR_CUDA, "launching ldma_kernel", e);
+        }
+    }
+    if (!rc && ((e = cudaMemcpyAsync(y, dy, njobs * nn * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+                (e = cudaMemcpyAsync(nodes, dn, njobs * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+                (e = cudaMemcpyAsync(status, ds, njobs * sizeof(int), cudaMemcpyDeviceToHost, st))))
+        rc = set_err(MGPU_ERR_CUDA, "copying LDMA results", e);
+    cudaFreeAsync(de, st);
+    cudaFreeAsync(dy, st);
+    cudaFreeAsync(dn, st);
+    cudaFreeAsync(ds, st);
+    if ((e = cudaStreamSynchronize(st)) && !rc) rc = set_err(MGPU_ERR_CUDA, "LDMA run", e);
+    return rc;
+}
+
+extern "C" void mgpu_ldma_destroy(mgpu_ldma *h) { delete h; }
+
 #include "server.cuh"

@@ -207,6 +207,61 @@ def mgprop(c: Coupling, sysm, rstart: float, dr: float, nstep: int, ered: float,
     return 0.5 * (y + y.T), nodes
 
 
+def maprop(c: Coupling, sysm, rstart: float, dr: float, nstep: int, ered: float, y0):
+    """MAPROP (maprop.f:33-290) restated: the quasi-adiabatic log-derivative
+    propagator.  Per sector: W at the midpoint (ERED = 0) diagonalised; the
+    first-order corrections (W(R_start) - W(R_mid)) DR/6 at the sector's start
+    and (W(R_end) - W(R_mid)) DR/6 carried from the previous end, added to Y
+    in the old adiabatic basis; Y turned into the new one (Q = T_old^T U); the
+    diagonal half-angle sector propagators of EIVAL - ERED; nodes from the
+    inversion unless a channel is deeper than 24/DR^2 (NCHECK).  Returns (Y
+    in the primitive basis, NODES)."""
+    n = c.n
+    eye = np.eye(n)
+    y = np.array(y0, dtype=np.float64)
+    t = eye.copy()
+    q = np.zeros((n, n))
+    r = rstart
+    u = hammat(c, r, sysm.pvec(r), 0.0)
+    nodes = 0
+    wmax = 24.0 / (dr * dr)
+    for k in range(nstep):
+        r = r + 0.5 * dr
+        w = hammat(c, r, sysm.pvec(r), 0.0)
+        corr = (u - w) * (dr / 6.0) + q
+        y = y + t.T @ corr @ t
+        ev, vec = np.linalg.eigh(w)
+        qm = t.T @ vec
+        t = vec
+        y = qm.T @ y @ qm
+        wref = ev - ered
+        flam = 0.5 * np.sqrt(np.abs(wref))
+        y1 = np.empty(n)
+        y2 = np.empty(n)
+        neg = wref < 0.0
+        tn = np.tan(flam[neg] * dr)
+        y1[neg] = flam[neg] / tn - flam[neg] * tn
+        y2[neg] = flam[neg] / tn + flam[neg] * tn
+        th = np.tanh(flam[~neg] * dr)
+        y1[~neg] = flam[~neg] / th + flam[~neg] * th
+        y2[~neg] = flam[~neg] / th - flam[~neg] * th
+        ncheck = int(np.sum(wref[~neg] > wmax))
+        inv, cnt = syminv(y + np.diag(y1))
+        if cnt > n:
+            raise RuntimeError(f"MAPROP: matrix inversion error at step {k + 1}")
+        inv = np.tril(inv) + np.tril(inv, -1).T
+        if rstart > rstart + dr:  # inward
+            cnt = n - cnt
+        if ncheck == 0:
+            nodes += cnt
+        y = -(y2[:, None] * inv * y2[None, :]) + np.diag(y1)
+        r = r + 0.5 * dr
+        u = hammat(c, r, sysm.pvec(r), 0.0)
+        q = (u - w) * (dr / 6.0)
+    y = t @ y @ t.T + q
+    return 0.5 * (y + y.T), nodes
+
+
 def radial_grid(rstart: float, dr: float, nstep: int) -> np.ndarray:
     """Radii in the order MDPROP/LDPROP visit them: R=RSTART, then R=R+H
     repeated (mdprop.f:69,117,203; ldprop.f:30,57,105)."""
@@ -646,6 +701,9 @@ def molscat_smatrix(sysm: Itype1, jtot: int, block: int, energies, rmin: float, 
             y, nodes, st, kf = mdprop(c, rtab, ptab, nstep, dr, ered, y0)
         elif propagator == "LDJ":
             y, nodes, st, kf = ldprop(c, rtab, ptab, nstep, dr, ered, y0)
+        elif propagator == "LDMA":
+            y, nodes = maprop(c, sysm, rstart, dr, nstep, ered, y0)
+            st, kf = 0, 0
         elif propagator in ("LDMG4", "LDMG5"):
             y, nodes = mgprop(c, sysm, rstart, dr, nstep, ered, y0, int(propagator[-1]))
             st, kf = 0, 0

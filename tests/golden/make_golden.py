@@ -17,7 +17,9 @@ examples/input/bound-basic1.input.
 
 Source: examples/output/molscat-all_propagators.output, runs
 "IPROPS=5" (LDPROP, lines 408-537), "IPROPS=6" (MDPROP, lines 682-811) and
-"IPROPS=8" (MGPROP with IMGSEL=5, the six-step MA5 method, lines 1231-1358):
+"IPROPS=8" (MGPROP with IMGSEL=5, the six-step MA5 method, lines 1231-1358)
+and "IPROPS=7" (MAPROP, the quasi-adiabatic log-derivative propagator,
+lines 956-1084):
 ITYPE=1, JTOT=10, symmetry block 1, N=12, E=1000 and 900 cm-1, 8072 steps.
 The system definition is examples/input/molscat-all_propagators.input:25-71.
 """
@@ -59,7 +61,7 @@ def main():
     with open(path) as f:
         runs = parse_runs(f.read())
     sel = {}
-    for label, key in (("IPROPS=6", "LDMD"), ("IPROPS=5", "LDJ"), ("IPROPS=8", "LDMG")):
+    for label, key in (("IPROPS=6", "LDMD"), ("IPROPS=5", "LDJ"), ("IPROPS=8", "LDMG"), ("IPROPS=7", "LDMA")):
         r = runs[label]
         sel[key] = {
             "energies_cm": [1000.0, 900.0],
@@ -71,7 +73,7 @@ def main():
         }
     doc = {
         "source": "examples/output/molscat-all_propagators.output (IPROPS=6 lines 682-811, IPROPS=5 lines 408-537, "
-                  "IPROPS=8 with IMGSEL=5 lines 1231-1358)",
+                  "IPROPS=8 with IMGSEL=5 lines 1231-1358, IPROPS=7 lines 956-1084)",
         "system": {
             "itype": 1, "ured": 20.0, "be": 30.0, "jlevel": [0, 2, 4, 6],
             "lambda": [0, 2], "terms": [[[1.0, -12, None], [-2.0, -6, None]], [[-0.2, -6, None]]],

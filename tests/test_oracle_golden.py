@@ -2,7 +2,8 @@
 
 examples/output/molscat-all_propagators.output prints the 6x6 open-channel
 S matrix to 14 significant digits for LDMD (IPROPS=6), LDJ (IPROPS=5) and
-the symplectic LDMG (IPROPS=8, IMGSEL=5: MA5),
+the symplectic LDMG (IPROPS=8, IMGSEL=5: MA5) and the quasi-adiabatic LDMA
+(IPROPS=7),
 ITYPE=1, JTOT=10, block 1, N=12, E=1000 and 900 cm-1 (fixture made by
 tests/golden/make_golden.py).  The restated MOLSCAT driver path (FINDRM,
 DRSET, YINIT, propagator, YTOK, KTOS) must reproduce them within 1e-8.
@@ -21,7 +22,7 @@ def _system(g):
                     terms=[[tuple(t) for t in tl] for tl in s["terms"]], rm=s["rm"], epsil=s["epsil"])
 
 
-@pytest.mark.parametrize("prop", ["LDMD", "LDJ", "LDMG"])
+@pytest.mark.parametrize("prop", ["LDMD", "LDJ", "LDMG", "LDMA"])
 def test_smatrix_matches_reference_output(golden, prop):
     s = golden["system"]
     run = golden["runs"][prop]
