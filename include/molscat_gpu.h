@@ -200,6 +200,22 @@ int mgpu_ldma_create(mgpu_ldma **out, int n, int nstep, double dr, int inward, c
 int mgpu_ldma_run_host(mgpu_ldma *h, int njobs, const double *ered, double *y, int *nodes, int *status);
 void mgpu_ldma_destroy(mgpu_ldma *h);
 
+/* ---- AIRY (the long-range propagator's sweep) ------------------------------
+ * aiprop.f:160-250 for many energies of one system, N <= 64: per sector k
+ * Z = T_k^T Z T_k, Z = Y4 - Y2 (Z + Y1)^-1 Y2 with NODES from the
+ * inversion's negative pivots (N - count for inward = 1), at the end
+ * V Z V^T.  The sector geometry (tmat[nsect][n*n]: previous local basis ->
+ * this one, the first from the primitive basis; vfin[n*n]: the last local
+ * basis) and, per energy, the diagonal sector functions
+ * y124[njobs][nsect][n][3] = (Y1, Y2, Y4) come from the host
+ * (molscat_b200.airy: the reference's first-energy geometry, Airy functions
+ * of the linear reference potential).  z[njobs][n*n]: Z at RSTART in the
+ * primitive basis in, at RSTOP out. */
+typedef struct mgpu_airy mgpu_airy;
+int mgpu_airy_create(mgpu_airy **out, int n, int nsect, int inward, const double *tmat, const double *vfin);
+int mgpu_airy_run_host(mgpu_airy *h, int njobs, const double *y124, double *z, int *nodes, int *status);
+void mgpu_airy_destroy(mgpu_airy *h);
+
 /* ---- Y -> K -> S on the device ---------------------------------------------
  * YTOK/YTOKG/KSYM (ytok.f:21-47, ytokg.f:71-126) and KTOS (ktos.f:149-169)
  * for every job after its propagation, at R = the grid's last radius: the

@@ -57,6 +57,7 @@ EXPORTS = (
     "mgpu_probe_pivot_reciprocal", "mgpu_mdprop_f", "mgpu_ldprop_f",
     "mgpu_plan_cancel", "mgpu_plan_set_time_limit", "mgpu_set_step_wait_limit", "mgpu_ldmg_radii",
     "mgpu_mgprop", "mgpu_mgprop_f", "mgpu_ldma_create", "mgpu_ldma_run_host", "mgpu_ldma_destroy",
+    "mgpu_airy_create", "mgpu_airy_run_host", "mgpu_airy_destroy",
 )
 
 _lib = None
@@ -83,6 +84,9 @@ def load(path: str | None = None):
                                    _dp, _dp, _dp, _dp, _dp]
     L.mgpu_ldma_run_host.argtypes = [vp, ctypes.c_int, _dp, _dp, _ip, _ip]
     L.mgpu_ldma_destroy.argtypes = [vp]
+    L.mgpu_airy_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp]
+    L.mgpu_airy_run_host.argtypes = [vp, ctypes.c_int, _dp, _dp, _ip, _ip]
+    L.mgpu_airy_destroy.argtypes = [vp]
     L.mgpu_plan_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, pc, pg, ctypes.c_int, _ip, _dp]
     L.mgpu_plan_destroy.argtypes = [vp]
     L.mgpu_plan_destroy.restype = None

@@ -160,5 +160,110 @@ ldma_kernel(Tables T, const double *__restrict__ ered, double *__restrict__ y, i
     }
 }
 
+// AIRY's sweep (aiprop.f:160-250) for the energies of one system: per
+// sector Z = T_k^T Z T_k (symmetrised), (Z + Y1)^-1 by the same unpivoted
+// Gauss-Jordan with its negative-pivot count (NODES += count outwards,
+// N - count inwards), Z = -Y2 (Z + Y1)^-1 Y2 + Y4; at the end V Z V^T.  The
+// sector functions (Y1, Y2, Y4) of every job, sector and channel come from
+// the host: y124[job][sector][channel][3].
+struct AiryTables {
+    int n, nsect, inward;
+    const double *tmat;  // [nsect][n*n] column-major
+    const double *vfin;  // [n*n]
+};
+
+__global__ void __launch_bounds__(kThreads)
+airy_kernel(AiryTables T, const double *__restrict__ y124, double *__restrict__ z, int *__restrict__ nodes_out,
+            int *__restrict__ status_out)
+{
+    extern __shared__ __align__(16) double airy_sm[];  // A and Z: n*n doubles each
+    __shared__ double s_r;
+    __shared__ int s_neg, s_bad;
+    const int n = T.n, nn = n * n, tid = threadIdx.x;
+    double *A = airy_sm, *Z = airy_sm + nn;
+    const int job = blockIdx.x;
+    const double *yj = y124 + (size_t)job * T.nsect * n * 3;
+    double *zj = z + (size_t)job * nn;
+    for (int x = tid; x < nn; x += kThreads) A[x] = zj[x];
+    if (tid == 0) s_bad = 0;
+    int nodes = 0, status = MGPU_OK;
+    __syncthreads();
+    for (int k = 0; k < T.nsect; ++k) {
+        const double *Q = T.tmat + (size_t)k * nn, *yk = yj + (size_t)k * n * 3;
+        gemm(A, Q, Z, n);  // Z T
+        __syncthreads();
+        for (int x = tid; x < nn; x += kThreads) {  // T^T (Z T)
+            const int i = x % n, j = x / n;
+            double v = 0.0;
+            for (int m = 0; m < n; ++m) v = fma(__ldg(Q + m + (size_t)i * n), Z[m + j * n], v);
+            A[x] = v;
+        }
+        if (tid == 0) s_neg = 0;
+        __syncthreads();
+        // symmetrised, plus Y1 on the diagonal
+        for (int x = tid; x < nn; x += kThreads) {
+            const int i = x % n, j = x / n;
+            Z[x] = 0.5 * (A[x] + A[j + i * n]) + (i == j ? __ldg(yk + 3 * i) : 0.0);
+        }
+        __syncthreads();
+        for (int p = 0; p < n; ++p) {
+            if (tid == 0) {
+                const double d = Z[p + p * n];
+                if (d < 0.0) ++s_neg;
+                if (d == 0.0 || !isfinite(d)) s_bad = d == 0.0 ? MGPU_ERR_INVERSION : MGPU_ERR_NONFINITE;
+                s_r = 1.0 / d;
+            }
+            __syncthreads();
+            const double r = s_r;
+            for (int x = tid; x < nn; x += kThreads) {
+                const int i = x % n, j = x / n;
+                if (i != p && j != p) A[x] = Z[x] - Z[i + p * n] * Z[p + j * n] * r;
+            }
+            __syncthreads();
+            for (int x = tid; x < nn; x += kThreads) {
+                const int i = x % n, j = x / n;
+                if (i == p && j == p) Z[x] = r;
+                else if (j == p) Z[x] = -Z[x] * r;
+                else if (i == p) Z[x] = Z[x] * r;
+                else Z[x] = A[x];
+            }
+            __syncthreads();
+        }
+        if (s_bad) {
+            status = s_bad;
+            break;
+        }
+        for (int x = tid; x < nn; x += kThreads) {
+            const int i = x % n, j = x / n;
+            const double zl = i >= j ? Z[x] : Z[j + i * n];
+            A[x] = -__ldg(yk + 3 * i + 1) * zl * __ldg(yk + 3 * j + 1) + (i == j ? __ldg(yk + 3 * i + 2) : 0.0);
+        }
+        nodes += T.inward ? n - s_neg : s_neg;
+        __syncthreads();
+    }
+    if (status == MGPU_OK) {
+        const double *V = T.vfin;
+        for (int x = tid; x < nn; x += kThreads) {  // Z = A V^T
+            const int i = x % n, j = x / n;
+            double v = 0.0;
+            for (int m = 0; m < n; ++m) v = fma(A[i + m * n], __ldg(V + j + (size_t)m * n), v);
+            Z[x] = v;
+        }
+        __syncthreads();
+        for (int x = tid; x < nn; x += kThreads) {  // V Z
+            const int i = x % n, j = x / n;
+            double v = 0.0;
+            for (int m = 0; m < n; ++m) v = fma(__ldg(V + i + (size_t)m * n), Z[m + j * n], v);
+            A[x] = v;
+        }
+        __syncthreads();
+        for (int x = tid; x < nn; x += kThreads) zj[x] = 0.5 * (A[x] + A[(x / n) + (x % n) * n]);
+    }
+    if (tid == 0) {
+        status_out[job] = status;
+        nodes_out[job] = status == MGPU_OK ? nodes : 0;
+    }
+}
+
 }  // namespace ldma
 }  // namespace mgpu

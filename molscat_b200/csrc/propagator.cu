@@ -2720,4 +2720,89 @@ extern "C" int mgpu_ldma_run_host(mgpu_ldma *h, int njobs, const double *ered, d
 
 extern "C" void mgpu_ldma_destroy(mgpu_ldma *h) { delete h; }
 
+// ---- AIRY's sweep for the energies of one system (sector tables from the host)
+struct mgpu_airy {
+    mgpu::ldma::AiryTables t{};
+    std::vector<void *> allocs;
+    cudaStream_t own = nullptr;
+    ~mgpu_airy()
+    {
+        if (own) cudaStreamSynchronize(own);
+        for (void *p : allocs) cudaFree(p);
+        if (own) cudaStreamDestroy(own);
+    }
+};
+
+extern "C" int mgpu_airy_create(mgpu_airy **out, int n, int nsect, int inward, const double *tmat, const double *vfin)
+{
+    if (!out) return set_err(MGPU_ERR_ARG, "null handle pointer");
+    *out = nullptr;
+    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "AIRY's sweep runs for 1 <= N <= 64");
+    if (nsect < 1 || !tmat || !vfin) return set_err(MGPU_ERR_ARG, "bad sector tables");
+    mgpu_airy *h = new (std::nothrow) mgpu_airy();
+    if (!h) return set_err(MGPU_ERR_NOMEM, "host allocation failed");
+    const size_t nn = (size_t)n * n;
+    const AllocFn al = [h](void **p, size_t nb) {
+        cudaError_t e = cudaMalloc(p, nb);
+        if (e == cudaSuccess) h->allocs.push_back(*p);
+        return e;
+    };
+    const UploadFn up = [](void *dst, const void *src, size_t nb) {
+        return cudaMemcpy(dst, src, nb, cudaMemcpyHostToDevice);
+    };
+    double *dt = nullptr, *dv = nullptr;
+    cudaError_t e;
+    if ((e = put_n(al, up, &dt, tmat, (size_t)nsect * nn)) || (e = put_n(al, up, &dv, vfin, nn)) ||
+        (e = cudaStreamCreateWithFlags(&h->own, cudaStreamNonBlocking))) {
+        delete h;
+        return set_err(MGPU_ERR_NOMEM, "uploading the AIRY tables", e);
+    }
+    h->t = mgpu::ldma::AiryTables{n, nsect, inward ? 1 : 0, dt, dv};
+    *out = h;
+    return MGPU_OK;
+}
+
+extern "C" int mgpu_airy_run_host(mgpu_airy *h, int njobs, const double *y124, double *z, int *nodes, int *status)
+{
+    if (!h) return set_err(MGPU_ERR_ARG, "null handle");
+    if (njobs < 0 || njobs > 65535) return set_err(MGPU_ERR_ARG, "0 <= jobs <= 65535");
+    if (njobs == 0) return MGPU_OK;
+    if (!y124 || !z || !nodes || !status) return set_err(MGPU_ERR_ARG, "null host buffer");
+    const size_t nn = (size_t)h->t.n * h->t.n, ny = (size_t)h->t.nsect * h->t.n * 3;
+    double *dy = nullptr, *dz = nullptr;
+    int *dn = nullptr, *ds = nullptr;
+    cudaError_t e;
+    cudaStream_t st = h->own;
+    if ((e = cudaMallocAsync((void **)&dy, njobs * ny * sizeof(double), st)) ||
+        (e = cudaMallocAsync((void **)&dz, njobs * nn * sizeof(double), st)) ||
+        (e = cudaMallocAsync((void **)&dn, njobs * sizeof(int), st)) ||
+        (e = cudaMallocAsync((void **)&ds, njobs * sizeof(int), st)))
+        return set_err(MGPU_ERR_NOMEM, "AIRY buffers", e);
+    int rc = MGPU_OK;
+    if ((e = cudaMemcpyAsync(dy, y124, njobs * ny * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(dz, z, njobs * nn * sizeof(double), cudaMemcpyHostToDevice, st)))
+        rc = set_err(MGPU_ERR_CUDA, "copying AIRY inputs", e);
+    if (!rc) {
+        const size_t sm = mgpu::ldma::smem_bytes(h->t.n);
+        if ((e = set_smem(mgpu::ldma::airy_kernel, sm))) {
+            rc = set_err(MGPU_ERR_CUDA, "airy_kernel set-up", e);
+        } else {
+            mgpu::ldma::airy_kernel<<<njobs, mgpu::ldma::kThreads, sm, st>>>(h->t, dy, dz, dn, ds);
+            if ((e = cudaGetLastError())) rc = set_err(MGPU_ERR_CUDA, "launching airy_kernel", e);
+        }
+    }
+    if (!rc && ((e = cudaMemcpyAsync(z, dz, njobs * nn * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+                (e = cudaMemcpyAsync(nodes, dn, njobs * sizeof(int), cudaMemcpyDeviceToHost, st)) ||
+                (e = cudaMemcpyAsync(status, ds, njobs * sizeof(int), cudaMemcpyDeviceToHost, st))))
+        rc = set_err(MGPU_ERR_CUDA, "copying AIRY results", e);
+    cudaFreeAsync(dy, st);
+    cudaFreeAsync(dz, st);
+    cudaFreeAsync(dn, st);
+    cudaFreeAsync(ds, st);
+    if ((e = cudaStreamSynchronize(st)) && !rc) rc = set_err(MGPU_ERR_CUDA, "AIRY run", e);
+    return rc;
+}
+
+extern "C" void mgpu_airy_destroy(mgpu_airy *h) { delete h; }
+
 #include "server.cuh"
