@@ -184,7 +184,7 @@ int mgpu_plan_run_device_phases(mgpu_plan *plan, double *y_dev, int *nodes_dev,
 
 /* ---- MAPROP (LDMA) ----------------------------------------------------------
  * The quasi-adiabatic log-derivative propagator (maprop.f:1-290, IPROP = 7)
- * for many energies of one system, N <= 64.  Its energy-independent half --
+ * for many energies of one system, N <= 100.  Its energy-independent half --
  * per sector k the eigenvalues EIVAL of W at the midpoint (with ERED = 0),
  * the basis change Q_k = T_{k-1}^T U_k and the first-order correction C_k
  * in the old basis, then the last basis T and end correction Q_end -- is
@@ -201,7 +201,7 @@ int mgpu_ldma_run_host(mgpu_ldma *h, int njobs, const double *ered, double *y, i
 void mgpu_ldma_destroy(mgpu_ldma *h);
 
 /* ---- AIRY (the long-range propagator's sweep) ------------------------------
- * aiprop.f:160-250 for many energies of one system, N <= 64: per sector k
+ * aiprop.f:160-250 for many energies of one system, N <= 100: per sector k
  * Z = T_k^T Z T_k, Z = Y4 - Y2 (Z + Y1)^-1 Y2 with NODES from the
  * inversion's negative pivots (N - count for inward = 1), at the end
  * V Z V^T.  The sector geometry (tmat[nsect][n*n]: previous local basis ->

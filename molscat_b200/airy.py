@@ -18,7 +18,7 @@ the host (`sector_tables`); per energy the eigenvalues shift by E - E0 and
 the host evaluates the Airy sector functions (`sector_y124`, O(N) a
 sector); the device runs the O(N^3) sweep: the basis change, the inversion
 with its negative-pivot count and the imbedding update
-(`mgpu_airy_run_host`, one CTA per energy, N <= 64).
+(`mgpu_airy_run_host`, one CTA per energy, N <= 100).
 """
 from __future__ import annotations
 
@@ -263,3 +263,35 @@ class AiryPlan:
             self.close()
         except Exception:
             pass
+
+
+class AiryInward:
+    """A long-range AIRY segment as the inward propagator of a BOUND/FIELD
+    search (`BoundProblem(inward=...)`): called with ERED it returns (Z at
+    RSTOP, NODES).  The sector geometry is built at the first energy it is
+    called with and kept for the later ones, as the reference's ISCRU file
+    keeps it; z0(ered) gives Z at RSTART (default: the adiabatic WKB start
+    for closed channels, bound.adiabatic_wkb_y)."""
+
+    def __init__(self, coupling: Coupling, potential, rstart: float, rstop: float, drnow: float,
+                 tolhi: float = 1.0e-4, powr: float = 3.0, nstep: int = 0, z0=None):
+        self.c, self.potential = coupling, potential
+        self.args = (rstart, rstop, drnow, tolhi, powr, nstep)
+        self.z0 = z0
+        self.plan = None
+
+    def __call__(self, ered: float):
+        rstart, rstop, drnow, tolhi, powr, nstep = self.args
+        if self.plan is None:
+            t = sector_tables(self.c, self.potential, rstart, rstop, drnow, float(ered), tolhi=tolhi, powr=powr,
+                              nstep=nstep)
+            self.plan = AiryPlan(t)
+        if self.z0 is not None:
+            z0 = self.z0(float(ered))
+        else:
+            from .bound import adiabatic_wkb_y
+            z0 = adiabatic_wkb_y(self.c, rstart, self.potential(rstart), float(ered), rstop > rstart)
+        zs, nodes, status = self.plan.run_host([z0], [float(ered)])
+        if status[0] != 0:
+            raise PropagatorError(f"AIRY: {_lib.status_string(int(status[0]))}", int(status[0]))
+        return zs[0], int(nodes[0])

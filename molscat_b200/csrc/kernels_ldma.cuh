@@ -1,6 +1,6 @@
 // MAPROP (maprop.f:33-290), the quasi-adiabatic log-derivative propagator,
 // for the energies of one system: one CTA per energy, Y dense in shared
-// memory (N <= 64).  Everything that does not depend on the energy -- the
+// memory (N <= 100).  Everything that does not depend on the energy -- the
 // adiabatic bases at the sector midpoints and their eigenvalues, the basis
 // changes Q_k = T_{k-1}^T U_k and the first-order corrections in the old
 // basis -- comes from tables the host builds once per system (what the
@@ -15,7 +15,7 @@
 namespace mgpu {
 namespace ldma {
 
-constexpr int kMaxN = 64;
+constexpr int kMaxN = 100;  // two n x n matrices in shared memory: 160 KB at 100
 constexpr int kThreads = 256;
 inline size_t smem_bytes(int n) { return 2 * (size_t)n * n * sizeof(double); }
 

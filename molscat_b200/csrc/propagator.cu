@@ -2648,7 +2648,7 @@ extern "C" int mgpu_ldma_create(mgpu_ldma **out, int n, int nstep, double dr, in
 {
     if (!out) return set_err(MGPU_ERR_ARG, "null handle pointer");
     *out = nullptr;
-    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "LDMA runs for 1 <= N <= 64");
+    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "LDMA runs for 1 <= N <= 100");
     if (nstep < 1 || !(dr != 0.0) || !std::isfinite(dr)) return set_err(MGPU_ERR_ARG, "bad NSTEP or DR");
     if (!eival || !q || !corr || !tfin || !qfin) return set_err(MGPU_ERR_ARG, "null table");
     mgpu_ldma *h = new (std::nothrow) mgpu_ldma();
@@ -2737,7 +2737,7 @@ extern "C" int mgpu_airy_create(mgpu_airy **out, int n, int nsect, int inward, c
 {
     if (!out) return set_err(MGPU_ERR_ARG, "null handle pointer");
     *out = nullptr;
-    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "AIRY's sweep runs for 1 <= N <= 64");
+    if (n < 1 || n > mgpu::ldma::kMaxN) return set_err(MGPU_ERR_UNSUPPORTED, "AIRY's sweep runs for 1 <= N <= 100");
     if (nsect < 1 || !tmat || !vfin) return set_err(MGPU_ERR_ARG, "bad sector tables");
     mgpu_airy *h = new (std::nothrow) mgpu_airy();
     if (!h) return set_err(MGPU_ERR_NOMEM, "host allocation failed");

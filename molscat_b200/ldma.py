@@ -16,7 +16,7 @@ once per system, in the order maprop.f:33-290 forms it:
 The energy-dependent sweep (the basis change of Y, the half-angle sector
 propagators of EIVAL - ERED, the inversion and its node count, the last
 back-transformation) runs on the device (`mgpu_ldma_run_host`, one CTA per
-energy, N <= 64).
+energy, N <= 100).
 """
 from __future__ import annotations
 

@@ -9,10 +9,11 @@ test_rb2.py, test_ytrans.py).
   device's sweep give the oracle's Z (1e-10 of max|Z|), NODES and sector
   count: outward and inward with TOLHI step control, and the TOLHI = 0
   series.
-* GPU: the device's sweep against the oracle on random systems; and
+* GPU: the device's sweep against the oracle on random systems;
   molscat-basic_Rb2 on product code alone -- MDPROP to 21 bohr and AIRY to
   15000 bohr on the device, YTRANS, YTOK and KTOS on the device -- giving
-  the printed s-wave scattering lengths.
+  the printed s-wave scattering lengths; bound-Mg_NH (N = 100) with the
+  product's AIRY inward, the printed bound states within DTOL.
 """
 import json
 import os
@@ -128,3 +129,27 @@ def test_gpu_rb2_scattering_lengths_on_product_code(gpu):
         TY._check_lengths(got, case.field(fg)["lengths"])
         ap.close()
         plan.close()
+
+
+@pytest.mark.gpu
+def test_gpu_bound_mg_nh_with_product_airy(gpu):
+    """bound-Mg_NH (N = 100) at 370 G: MDPROP outward on the device and
+    AIRY inward (RMAX = 50 -> RMATCH = 7 bohr, TOLHI = 1e-6) through
+    AiryInward, its geometry from the first energy of the search as the
+    reference's ISCRU = 30 run keeps it: the printed states within DTOL."""
+    import test_mg_nh as MG
+    from molscat_b200.bound import BoundProblem, find_states_converged
+    with open(os.path.join(HERE, "golden", "bound_mg_nh.json")) as f:
+        g = json.load(f)
+    st = g["sets"][0]
+    s = g["system"]
+    run = MG._Run(g, st["field"])
+    inward = AY.AiryInward(run.c, run.sysm.pvec, s["rmax"], s["rmatch"], -s["drl"], tolhi=s["tolhil"], powr=3.0)
+    bp = BoundProblem(run.c, run.seg_out, prop="LDMD", inward=inward)
+    tol, coarse = run.tolerances()
+    res, _ = find_states_converged(bp, run.ered(s["emin_mhz"]), run.ered(s["emax_mhz"]), tol, coarse)
+    assert len(res) == len(st["states"])
+    for (k, e, _, _), ref in zip(res, st["states"]):
+        assert k + 1 == ref["state"]
+        assert abs(run.to_mhz(e) - ref["energy_mhz"]) < s["dtol_mhz"]
+
