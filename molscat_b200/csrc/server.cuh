@@ -181,7 +181,7 @@ int mgpu_server::launch(Slot &sl, const std::vector<long long> &tickets, const s
         for (const JobDev &jd : jobs) mx = std::max(mx, sys_nstep[jd.sys]);
         const int rc = setup_big(g, iprop, b, jobs.data(), j_dev, M, mx, {}, hs, sys_n, sys_nstep, d_prep, al, up);
         if (rc) return rc;
-        e = run_big_prop(g, iprop, d_sys, y_dev, nodes, status, kfail, st, sl.side, sl.evf, sl.evj);
+        e = run_big_prop(g, iprop, d_sys, y_dev, nodes, status, kfail, st, BigAux{sl.side, sl.evf, sl.evj});
         sl.graph = g.step_graph;  // destroyed when the batch retires
         if (e) return set_err(MGPU_ERR_CUDA, "large-N batch", e);
     } else {
@@ -481,7 +481,7 @@ int mgpu_server_add_system(mgpu_server *s, const mgpu_coupling *c, const mgpu_gr
             BigBucket gb;
             rc = setup_big(gb, s->iprop, b, nullptr, nullptr, 0, 0, {sid}, s->hs, s->sys_n, s->sys_nstep, s->d_prep,
                            tal, up);
-            if (!rc && (e = run_big_prep(gb, s->d_sys, s->sys_nstep, s->reg, s->reg_side, s->reg_evf, s->reg_evj)))
+            if (!rc && (e = run_big_prep(gb, s->d_sys, s->sys_nstep, s->reg, BigAux{s->reg_side, s->reg_evf, s->reg_evj})))
                 rc = set_err(MGPU_ERR_CUDA, "large-N preparation", e);
             cudaStreamSynchronize(s->reg);
             for (void *q : tmp) cudaFree(q);
